@@ -1,0 +1,248 @@
+/*
+ * gpufoam_b200 — C ABI of the B200 (sm_100a) per-cell detailed-chemistry solver.
+ *
+ * This is the drop-in seam for the OpenFOAM `gpuChemistryModel` plugin of gpuFoam.
+ * The plugin keeps its OpenFOAM side (dictionary loaders, field gather/scatter,
+ * `solve(deltaT)` contract); everything below `FoamGpu::GpuKernelEvaluator` is
+ * replaced by the entry points declared here.
+ *
+ * Conventions
+ *   - Plain C types, pointers and sizes only. Every function returns an int
+ *     status (GF_OK == 0); no exception ever crosses this boundary.
+ *   - All arithmetic is IEEE FP64 (the reference's gScalar = double,
+ *     gpu_utils/common/gpu_constants.H:8); indices are int (gLabel).
+ *   - nEqns = nSpecie + 2; a cell state is [Y_0 .. Y_{nS-1}, T, p], cell-major
+ *     (the reference's Yvf layout, gpuChemistryModel.C:33-53).
+ *   - `stream` arguments are cudaStream_t passed as void* (0 = legacy default).
+ *
+ * Reference interfaces replaced (paths relative to the gpuFoam repository):
+ *   gf_thermo_from_nasa      makeGpuThermo            gpu_chemistry/src/gpuThermo/makeGpuThermo.H:16-48
+ *   gf_reaction_thermo       set_reaction_thermo      gpu_chemistry/src/gpuReaction/makeGpuReactions.H:18-59
+ *   gf_mech_create           thermosAndReactions ctor gpu_chemistry/src/gpuKernelEvaluator/gpuKernelEvaluator/thermosAndReactions.cu:10-24
+ *   gf_solver_create         GpuKernelEvaluator ctor  gpu_chemistry/src/gpuKernelEvaluator/gpuKernelEvaluator/gpuKernelEvaluator.cu:14-33
+ *                            + make_gpuODESolver      gpu_chemistry/src/gpuOde/makeGpuOdeSolver.H:13-31
+ *   gf_compute_rr            GpuKernelEvaluator::computeRR   gpuKernelEvaluator.cu:65-97
+ *   gf_compute_ynew          GpuKernelEvaluator::computeYNew gpuKernelEvaluator.cu:35-63
+ *   gf_solve                 computeYNew + computeRR on device memory (same contract, no host staging)
+ *   gf_rates                 gpuODESystem::derivatives      gpu_chemistry/src/gpuOde/gpuODESystem.H:164-196
+ *   gf_jacobian              gpuODESystem::jacobian         gpu_chemistry/src/gpuOde/gpuODESystem.H:198-281
+ *   gf_lu_decompose          LUDecompose                    gpu_chemistry/src/gpuOde/ludecompose.H:9-92
+ *   gf_lu_backsubstitute     LUBacksubstitute               gpu_chemistry/src/gpuOde/ludecompose.H:94-130
+ */
+#ifndef GPUFOAM_B200_H
+#define GPUFOAM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GF_ABI_VERSION 1
+
+/* Longest side of a reaction (reference MAX_REACTION_WIDTH, gpuReaction.H:12). */
+#define GF_MAX_REACTION_WIDTH 10
+/* Largest mechanism the kernels accept (nSpecie). The reference's third-body
+ * efficiency arrays hold 300 species (gpuThirdBodyEfficiencies.H:10). */
+#define GF_MAX_SPECIES 300
+
+/* ---- status codes ------------------------------------------------------ */
+enum gf_status {
+    GF_OK = 0,
+    GF_ERR_INVALID_ARGUMENT = 1,  /* null pointer, negative size, bad enum      */
+    GF_ERR_UNKNOWN_SOLVER = 2,    /* ode name not Rosenbrock12/23/34
+                                     (reference throws logic_error, makeGpuOdeSolver.H:28) */
+    GF_ERR_UNSUPPORTED = 3,       /* mechanism outside the kernels' limits        */
+    GF_ERR_MASS_IMBALANCE = 4,    /* |lhs - rhs| > 0.1 kg/kmol (makeGpuReactions.H:48-54) */
+    GF_ERR_CUDA = 5,              /* a CUDA runtime call failed                   */
+    GF_ERR_NO_DEVICE = 6,         /* no CUDA device visible                       */
+    GF_ERR_OUT_OF_MEMORY = 7,
+    GF_ERR_CELL_FAILURE = 8       /* at least one cell ended with a non-OK cell status */
+};
+
+/* Per-cell integration status (written to the optional `status` array). The
+ * reference traps on step underflow (gpuAdaptiveSolver.H:111-114) and returns
+ * silently on maxSteps (gpuODESolverBase.H:80-111); here both are reported. */
+enum gf_cell_status {
+    GF_CELL_OK = 0,
+    GF_CELL_STEP_UNDERFLOW = 1,   /* dx < vSmall during step rejection           */
+    GF_CELL_MAX_STEPS = 2,        /* maxSteps substeps taken before reaching deltaT */
+    GF_CELL_NONFINITE = 3,        /* NaN/Inf in the integrated state             */
+    GF_CELL_SKIPPED = 4           /* T <= Treact: chemistry not solved (not an error) */
+};
+
+/* Reaction-rate kinds (gpuReactionRate variant, gpuReactionRate.H:16-28). */
+enum gf_rate_type {
+    GF_RATE_ARRHENIUS = 0,             /* gpuArrheniusReactionRate              */
+    GF_RATE_THIRD_BODY_ARRHENIUS = 1,  /* gpuThirdBodyArrheniusReactionRate     */
+    GF_RATE_LINDEMANN_FALLOFF = 2,     /* gpuFallOffReactionRate<Arrhenius, Lindemann> */
+    GF_RATE_TROE_FALLOFF = 3           /* gpuFallOffReactionRate<Arrhenius, Troe>      */
+};
+
+enum gf_ode_kind { GF_ROSENBROCK12 = 12, GF_ROSENBROCK23 = 23, GF_ROSENBROCK34 = 34 };
+
+/* ---- mechanism description ---------------------------------------------- */
+
+/* One gpuThermo (gpuThermo.H:9-62): perfect gas (Y, W) + JANAF/NASA-7 with
+ * coefficients ALREADY multiplied by R = RR/W, as makeGpuThermo produces. */
+typedef struct gf_thermo {
+    double Y;
+    double W;
+    double Tlow, Thigh, Tcommon;
+    double high[7];
+    double low[7];
+} gf_thermo;
+
+/* gpuSpecieCoeffs (gpuReaction.H:25-37). `integer_exponent` != 0 selects the
+ * integerPow path with exponent (int)exponent (gpuSpecieExponent.H:103-110). */
+typedef struct gf_specie_coeff {
+    int index;
+    int integer_exponent;
+    double stoich;
+    double exponent;
+} gf_specie_coeff;
+
+/* One gpuReaction (gpuReaction.H:43-98). `thermo` is the reaction ΔThermo
+ * (the gpuThermo base of gpuReaction, set by set_reaction_thermo). */
+typedef struct gf_reaction {
+    gf_thermo thermo;
+    int n_lhs, n_rhs;
+    gf_specie_coeff lhs[GF_MAX_REACTION_WIDTH];
+    gf_specie_coeff rhs[GF_MAX_REACTION_WIDTH];
+    int rate_type;           /* enum gf_rate_type                                */
+    int irreversible;
+    /* Arrhenius, third-body Arrhenius, or the k0 of a fall-off rate */
+    double A, beta, Ta;
+    /* kInf of a fall-off rate (ignored otherwise) */
+    double Ainf, betainf, Tainf;
+    /* Troe F (gpuTroeFallOffFunction.H:10-25): alpha, T***, T*, T** */
+    double troe_alpha, troe_Tsss, troe_Ts, troe_Tss;
+    /* third-body efficiencies, nSpecie values; NULL for plain Arrhenius */
+    const double* efficiencies;
+    /* temperature limits of the rate (gpuReaction::Tlow/Thigh) */
+    double Tlow, Thigh;
+} gf_reaction;
+
+typedef struct gf_mech_desc {
+    int n_species;
+    int n_reactions;
+    const gf_thermo* thermos;       /* n_species   */
+    const gf_reaction* reactions;   /* n_reactions */
+} gf_mech_desc;
+
+/* gpuODESolverInputs (gpuODESolverInputs.H:9-23) with the solver name as an enum. */
+typedef struct gf_ode_inputs {
+    int solver;              /* enum gf_ode_kind */
+    double absTol, relTol;
+    int maxSteps;
+    double safeScale, alphaInc, alphaDec, minScale, maxScale;
+} gf_ode_inputs;
+
+/* Kernel launch form. kind: 0 = plain (one thread per cell, one launch over all
+ * cells, the reference's launch model); 1 = persistent work queue. */
+typedef struct gf_launch_config {
+    int kind;
+    int threads_per_cell;    /* 1, 2, 4, 8, 16 or 32 (persistent only)          */
+    int scratch_in_shared;   /* 1: per-cell workspace in shared memory           */
+    int cells_per_block;     /* groups per CTA (persistent only)                 */
+    int blocks_per_sm;       /* 0 = as many as fit                               */
+    int lu_block;            /* reserved, 0                                      */
+} gf_launch_config;
+
+typedef struct gf_stats {
+    long long accepted_steps;   /* summed over cells */
+    long long attempts;         /* accepted + rejected Rosenbrock attempts       */
+    long long failed_cells;     /* cells with a status other than OK/SKIPPED     */
+    double min_delta_t;         /* min over cells of deltaTChemNew before clamping */
+} gf_stats;
+
+typedef struct gf_mech gf_mech;
+typedef struct gf_solver gf_solver;
+
+/* ---- host helpers: the reference's mechanism loader arithmetic ---------- */
+
+/* makeGpuThermo (makeGpuThermo.H:16-48): coefficients × R where R = RR/W. */
+int gf_thermo_from_nasa(double Y, double W, double Tlow, double Thigh, double Tcommon,
+                        const double high_raw[7], const double low_raw[7], gf_thermo* out);
+
+/* set_reaction_thermo (makeGpuReactions.H:18-59): the reaction ΔThermo from the
+ * species thermos, with the same operator sequence (gpuThermo.H:352-470,
+ * gpuPerfectGas.H:100-117,280-325). Returns GF_ERR_MASS_IMBALANCE when the
+ * reference would raise its FatalError. */
+int gf_reaction_thermo(const gf_thermo* species, int n_species,
+                       int n_lhs, const gf_specie_coeff* lhs,
+                       int n_rhs, const gf_specie_coeff* rhs, gf_thermo* out);
+
+/* ---- mechanism / solver objects ----------------------------------------- */
+
+/* Copies the description into device tables on the current device. */
+int gf_mech_create(const gf_mech_desc* desc, gf_mech** out);
+void gf_mech_destroy(gf_mech* mech);
+int gf_mech_info(const gf_mech* mech, int* n_species, int* n_reactions, long long* device_bytes);
+
+/* One or more mechanisms (mixed batches address them by a per-cell id). */
+int gf_solver_create(const gf_mech* const* mechs, int n_mechs, const gf_ode_inputs* inputs,
+                     double Treact, gf_solver** out);
+void gf_solver_destroy(gf_solver* solver);
+int gf_solver_set_launch(gf_solver* solver, const gf_launch_config* cfg);
+int gf_solver_get_launch(const gf_solver* solver, gf_launch_config* cfg);
+
+/* ---- the per-flow-step solve --------------------------------------------- */
+
+/* Device-memory form of computeYNew + computeRR. All pointers are device pointers.
+ *   n_cells
+ *   deltaT         flow time step (used when deltaT_cell is NULL)
+ *   deltaT_cell    per-cell time step [n_cells] or NULL (local time stepping)
+ *   deltaTChemMax  clamp for the returned chemistry time steps
+ *   mech_id        per-cell mechanism index [n_cells] or NULL (all mechanism 0)
+ *   rho            old-time density [n_cells] (may be NULL when RR is NULL)
+ *   Y0             input states [n_cells][nEqns of the cell's mechanism], row stride ld_y
+ *   Ynew           output states, same layout (may alias Y0, may be NULL)
+ *   deltaTChem     in: chemistry time steps; out: new, clamped ≤ deltaTChemMax
+ *   RR             output rho*(Ynew-Y0)/deltaT [n_cells][ld_rr] or NULL
+ *   status         per-cell gf_cell_status [n_cells] or NULL
+ *   counters       per-cell accepted/attempt counts [n_cells][2] (int) or NULL
+ *   stats          host struct filled after the solve, or NULL (no host sync)
+ */
+int gf_solve(gf_solver* solver, int n_cells, double deltaT, const double* deltaT_cell,
+             double deltaTChemMax, const int* mech_id, const double* rho,
+             const double* Y0, int ld_y, double* Ynew, double* deltaTChem,
+             double* RR, int ld_rr, int* status, int* counters, gf_stats* stats,
+             void* stream);
+
+/* Host-memory mirror of GpuKernelEvaluator::computeRR (single mechanism):
+ * RR [n_cells][nSpecie], deltaTChemNew [n_cells] (clamped), *minDeltaT (before
+ * clamping). Copies in and out through pinned staging owned by the solver. */
+int gf_compute_rr(gf_solver* solver, int n_cells, double deltaT, double deltaTChemMax,
+                  const double* rho, const double* deltaTChem, const double* Y,
+                  double* RR, double* deltaTChemNew, double* minDeltaT);
+
+/* Host-memory mirror of GpuKernelEvaluator::computeYNew: Ynew [n_cells][nEqns]
+ * and deltaTChemNew [n_cells] (not clamped, as in the reference). */
+int gf_compute_ynew(gf_solver* solver, int n_cells, double deltaT, double deltaTChemMax,
+                    const double* deltaTChem, const double* Y, double* Ynew,
+                    double* deltaTChemNew);
+
+/* ---- parity entry points (one thread group per state, device pointers) --- */
+
+/* dydx [n_states][nEqns] = derivatives(y [n_states][nEqns]). */
+int gf_rates(const gf_mech* mech, int n_states, const double* y, double* dydx, void* stream);
+
+/* dfdx [n_states][nEqns] and J [n_states][nEqns][nEqns] = jacobian(y). */
+int gf_jacobian(const gf_mech* mech, int n_states, const double* y, double* dfdx,
+                double* J, void* stream);
+
+/* In-place LU of n_mats matrices [n_mats][m][m] with pivots [n_mats][m]. */
+int gf_lu_decompose(int n_mats, int m, double* A, int* pivots, void* stream);
+/* In-place solve of b [n_mats][m] with the factors from gf_lu_decompose. */
+int gf_lu_backsubstitute(int n_mats, int m, const double* LU, const int* pivots,
+                         double* b, void* stream);
+
+/* ---- misc --------------------------------------------------------------- */
+const char* gf_strerror(int status);
+int gf_abi_version(void);
+/* CUDA error text of the last GF_ERR_CUDA on this thread. */
+const char* gf_last_cuda_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUFOAM_B200_H */

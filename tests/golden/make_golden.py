@@ -1,0 +1,94 @@
+"""Generate the golden fixtures of tests/golden/ from the gpuFoam reference.
+
+Run in a container where the reference tree exists (its FP64 headers are
+compiled in place by oracle/Makefile into oracle/_ref/libgf_ref.so):
+
+    python tests/golden/make_golden.py
+
+Every expected value in the .npz files below comes from the reference's own
+code (gpuThermo, gpuReaction, gpuODESystem, LUDecompose/LUBacksubstitute,
+gpuRosenbrock12/23/34, odeSolve, singleCellSolver), evaluated on seeded
+synthetic mechanisms and cell states. The raw mechanism is stored with the
+results so that the fixtures do not depend on the generator staying unchanged.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from gpufoam_b200 import mechanism as M  # noqa: E402
+from oracle.oracle import Oracle, flatten, lu, ode_inputs  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+CASES = [
+    # name, mechanism factory, n states, n cells per solver, deltaT
+    ("h2size", M.h2_size, 8, 32, 1e-5),
+    ("coverage", M.coverage, 8, 32, 1e-5),
+    ("grisize", M.gri_size, 6, 12, 1e-6),
+]
+
+
+def make_case(name, factory, n_states, n_cells, deltaT):
+    mech = factory(0)
+    ref = Oracle(mech, "reference")
+    fl = flatten(mech)
+    out = {f"mech_{k}": np.asarray(v) for k, v in fl.items()}
+    sp, rx, ie = ref.tables()
+    out.update(species_tables=sp, reaction_tables=rx, int_exponents=ie, constants=ref.constants())
+    out["thermo_700"] = ref.thermo_eval(101325.0, 700.0)
+    out["thermo_1500"] = ref.thermo_eval(101325.0, 1500.0)
+    states = M.make_cells(mech, n_states, seed=11)
+    out["states"] = states
+    out["reaction_eval"] = np.stack([ref.reaction_eval(s) for s in states[:2]])
+    out["dydx"] = ref.derivatives(states)
+    dfdx, J = ref.jacobian(states)
+    out["dfdx"], out["J"] = dfdx, J
+    rng = np.random.default_rng(5)
+    dxs = 10.0 ** rng.uniform(-10, -7, size=n_states)
+    out["attempt_dx"] = dxs
+    for s in (12, 23, 34):
+        y, err = ref.attempt(ode_inputs(s), states, out["dydx"], dxs)
+        out[f"attempt{s}_y"], out[f"attempt{s}_err"] = y, err
+    cells = M.make_cells(mech, n_cells, seed=12)
+    out["cells"] = cells
+    out["deltaT"] = np.array(deltaT)
+    out["deltaTChem0"] = np.array(1e-7)
+    for s in (12, 23, 34):
+        Y, dtc, counts, _ = ref.cells(ode_inputs(s), cells, deltaT, 1e-7)
+        out[f"cells{s}_Y"], out[f"cells{s}_dtc"], out[f"cells{s}_counts"] = Y, dtc, counts
+    # the Treact gate: half of the cells below the threshold
+    Treact = float(np.median(cells[:, -2]))
+    Y, dtc, counts, _ = ref.cells(ode_inputs(34), cells, deltaT, 1e-7, Treact=Treact)
+    out["treact"] = np.array(Treact)
+    out["cells34_treact_Y"], out["cells34_treact_dtc"] = Y, dtc
+    # host computeRR arithmetic on the R34 result
+    rho = np.linspace(0.2, 1.3, n_cells)
+    RR, dtc_new, mn = ref.compute_rr_host(deltaT, 5e-8, rho, cells, out["cells34_Y"], out["cells34_dtc"])
+    out.update(rr_rho=rho, rr_RR=RR, rr_dtc=dtc_new, rr_min=np.array(mn), rr_dtcmax=np.array(5e-8))
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **out)
+    print(name, "written", {k: v.shape for k, v in out.items() if hasattr(v, "shape") and v.size > 50})
+
+
+def make_lu():
+    rng = np.random.default_rng(3)
+    out = {}
+    out["sizes"] = np.array([3, 4, 5, 7, 10, 12, 16, 24, 33, 49, 54])
+    for m in out["sizes"]:
+        A = rng.uniform(size=(1, m, m))
+        b = np.ones((1, m))
+        LU, piv, x = lu("reference", A, b)
+        out[f"A{m}"], out[f"LU{m}"], out[f"piv{m}"], out[f"x{m}"] = A, LU, piv, x
+    np.savez_compressed(os.path.join(OUT, "lu.npz"), **out)
+    print("lu written")
+
+
+if __name__ == "__main__":
+    make_lu()
+    for case in CASES:
+        make_case(*case)
