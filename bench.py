@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Benchmark: cells/s per flow step (ΔT) of the per-cell chemistry solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload gri-100k|gri-bimodal-1M|h2-1k|mixed-750k] [--solver 34]
+                    [--no-plain] [--no-e2e] [--no-cpu]
+
+A step is one gf_solve over the whole batch: every cell integrated over one
+flow time step ΔT with adaptive Rosenbrock substeps, relTol 1e-4, absTol 1e-8,
+starting each step from the same states and deltaTChem = 1e-7 s (the
+reference tutorials' initialChemicalTimeStep). Inputs are seeded synthetic
+batches larger than L2 (126 MB) for the GPU workloads.
+
+`value`     persistent work-queue kernel, inputs resident in HBM, CUDA events
+`plain`     the one-thread-per-cell kernel on the same batch (the reference's
+            launch model), for the persistent-vs-plain ratio
+`e2e`       GpuKernelEvaluator.computeRR through the C ABI from pinned host
+            arrays: H2D of Y/ΔTChem/rho, the solve, D2H of RR/ΔTChem
+`roofline`  FP64 pipe: algorithmic FLOP (gpufoam_b200/flops.py) per launch ÷
+            launch time, against the DFMA peak measured live on this GPU
+`cpu_baseline` the reference's own FP64 code (compiled in place, OpenMP over
+            cells on all host cores) on a bounded sample of the same batch
+
+Multi-GPU (torchrun): every rank integrates its own batch of the workload's
+size (weak scaling, cells are independent); the one exchange per step is the
+min over ranks of the new chemistry time step (NCCL all-reduce).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: mechanism, cells, deltaT, T sampling
+    "h2-1k": dict(mech="h2", n=1024, dT=1e-5, T=(1000.0, 2500.0)),
+    "gri-100k": dict(mech="gri", n=100_000, dT=1e-6, T=(1000.0, 2500.0)),
+    "gri-bimodal-1M": dict(mech="gri", n=1_000_000, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0))),
+    # small cases of the same kernels, for ncu captures and launch sweeps
+    "gri-4k": dict(mech="gri", n=4096, dT=1e-6, T=(1000.0, 2500.0)),
+    "gri-16k": dict(mech="gri", n=16384, dT=1e-6, T=(1000.0, 2500.0)),
+}
+DTC0 = 1e-7
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="gri-100k", choices=list(WORKLOADS))
+    ap.add_argument("--solver", type=int, default=34, choices=[12, 23, 34])
+    ap.add_argument("--launch", default="fixed", choices=["fixed", "auto", "sweep"],
+                    help="fixed: --threads-per-cell/--shared; auto: autotuner on a sample; "
+                         "sweep: print every launch form's time to stderr, then use the best")
+    ap.add_argument("--threads-per-cell", type=int, default=32)
+    ap.add_argument("--shared", type=int, default=1)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def make_batch(wl, seed):
+    from gpufoam_b200 import mechanism as M
+    raw = M.h2_size(0) if wl["mech"] == "h2" else M.gri_size(0)
+    if "bimodal" in wl:
+        cells = M.make_cells(raw, wl["n"], seed=seed, bimodal=wl["bimodal"])
+    else:
+        cells = M.make_cells(raw, wl["n"], seed=seed, T_range=wl["T"])
+    return raw, cells
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, device_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(device_index)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_rate(raw, cells, solver, dT, seconds, nthreads):
+    """The reference's own singleCellSolver (oracle/_ref) over a bounded
+    sample of cells with all host threads; returns (cells/s, sample size, kind)."""
+    from oracle.oracle import REF_LIB, Oracle, ode_inputs
+    kind = "reference" if os.path.exists(REF_LIB) else "port"
+    o = Oracle(raw, kind)
+    inp = ode_inputs(solver)
+    n = max(nthreads * 4, 32)
+    done, t_total = 0, 0.0
+    while t_total < seconds and done < cells.shape[0]:
+        chunk = cells[done:done + n]
+        t0 = time.perf_counter()
+        if kind == "reference":
+            o.cells_uncounted(inp, chunk, dT, DTC0, nthreads=nthreads)
+        else:
+            o.cells(inp, chunk, dT, DTC0, nthreads=nthreads)
+        t_total += time.perf_counter() - t0
+        done += chunk.shape[0]
+        n = min(n * 2, 4096)
+    return done / t_total, done, kind, t_total
+
+
+def main():
+    args = parse()
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nthreads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        raw, cells = make_batch(wl, seed=1000)
+        times = []
+        sample = None
+        rates = []
+        for k in range(args.warmup + args.steps):
+            r, done, kind, t = cpu_reference_rate(raw, cells[(k * 997) % max(1, cells.shape[0] - 4096):], args.solver,
+                                                  wl["dT"], max(2.0, args.cpu_seconds / 4), nthreads)
+            if k >= args.warmup:
+                rates.append(r)
+                times.append(t)
+                sample = done
+        value = float(np.mean(rates))
+        line = {"impl": "reference", "metric": f"cells/s per ΔT at relTol 1e-4 ({args.workload}, R{args.solver})",
+                "value": value, "unit": "cells/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "cells": wl["n"], "deltaT": wl["dT"],
+                           "solver": f"Rosenbrock{args.solver}", "relTol": 1e-4, "absTol": 1e-8},
+                "cpu_baseline": {"value": value, "unit": "cells/s", "cores": nthreads, "kind": kind,
+                                 "sample": f"{sample} cells of the {args.workload} batch per step, OpenMP "
+                                           f"schedule(dynamic,64) over cells"},
+                "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from gpufoam_b200 import _native as N
+    from gpufoam_b200 import evaluator as E
+    from gpufoam_b200 import flops as F
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    raw, cells = make_batch(wl, seed=1000 + rank)
+    n = cells.shape[0]
+    mech = E.Mechanism(raw)
+    ode = E.OdeInputs(f"Rosenbrock{args.solver}", absTol=1e-8, relTol=1e-4)
+    Y0 = torch.as_tensor(cells, device="cuda")
+    dtc0 = torch.full((n,), DTC0, dtype=torch.float64, device="cuda")
+    dtc = dtc0.clone()
+    Ynew = torch.empty_like(Y0)
+    counters = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+    lib = N.load()
+
+    def timed(solver, steps, warmup):
+        stream = torch.cuda.current_stream()
+        for _ in range(warmup):
+            dtc.copy_(dtc0)
+            solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, want_status=False, want_counters=False, want_stats=False)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = []
+        launches = 0
+        for _ in range(steps):
+            dtc.copy_(dtc0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, want_status=False, want_counters=True,
+                               want_stats=False)
+            e1.record(stream)
+            launches += 2  # queue reset + the solve kernel
+            if world > 1:
+                # the exchange of the step: min over ranks of the new chemistry time step
+                mn = dtc.min().reshape(1)
+                dist.all_reduce(mn, op=dist.ReduceOp.MIN)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        cnt = out["counters"].cpu().numpy()
+        return ms, cnt, launches
+
+    # FP64 roofline denominator, measured on this GPU
+    import ctypes
+    peak = ctypes.c_double()
+    N.check(lib.gf_measure_fp64_peak(200.0, ctypes.byref(peak)), "gf_measure_fp64_peak")
+
+    solver = E.Solver([mech], ode)
+    solver.set_launch(kind=1, threads_per_cell=args.threads_per_cell, scratch_in_shared=args.shared)
+    tuned = None
+    if args.launch != "fixed":
+        from gpufoam_b200 import autotune
+        rng = np.random.default_rng(7)
+        sample = cells[rng.choice(n, size=min(n, 8192), replace=False)]
+        tuned = autotune.tune(solver, sample, wl["dT"], DTC0, use_cache=(args.launch == "auto"),
+                              verbose=False)
+        if args.launch == "sweep" and rank == 0:
+            for cfg, ms in tuned["table"]:
+                print(json.dumps({"sweep": cfg, "ms": ms, "cells": int(sample.shape[0])}), file=sys.stderr)
+    clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    ms, cnt, launches = timed(solver, args.steps, args.warmup)
+    clk = clocks.stop() if clocks else None
+    ms_step = float(np.mean(ms))
+    t_max = ms_step
+    if world > 1:
+        t = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * n / (t_max * 1e-3)
+    attempts, accepted = int(cnt[:, 1].sum()), int(cnt[:, 0].sum())
+    flop = F.total(raw, args.solver, attempts, accepted)
+    achieved = flop / (ms_step * 1e-3) / 1e12
+
+    plain = None
+    if not args.no_plain:
+        ps = E.Solver([mech], ode)
+        ps.set_launch(kind=0)
+        pms, pcnt, _ = timed(ps, max(1, min(args.steps, 2)), 1)
+        pm = float(np.mean(pms))
+        if world > 1:
+            t = torch.tensor([pm], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pm = float(t.item())
+        plain = {"value": world * n / (pm * 1e-3), "ms_per_step": pm, "unit": "cells/s",
+                 "launch": "one thread per cell, HBM scratch"}
+        del ps
+
+    e2e = None
+    if not args.no_e2e:
+        ev = E.GpuKernelEvaluator(n, raw.n_eqns, raw.n_species, mech, ode)
+        ev.solver.set_launch(kind=1, threads_per_cell=args.threads_per_cell, scratch_in_shared=args.shared)
+        hY = torch.empty((n, raw.n_eqns), dtype=torch.float64, pin_memory=True)
+        hY.copy_(torch.as_tensor(cells))
+        hrho = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        hrho.copy_(torch.as_tensor(np.linspace(0.2, 1.2, n)))
+        hdtc = torch.full((n,), DTC0, dtype=torch.float64).pin_memory()
+        ev.computeRR(wl["dT"], 1.0, hrho.numpy(), hdtc.numpy(), hY.numpy())
+        em = []
+        for _ in range(max(1, min(args.steps, 2))):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            RR, dtn, mn = ev.computeRR(wl["dT"], 1.0, hrho.numpy(), hdtc.numpy(), hY.numpy())
+            e1.record()
+            torch.cuda.synchronize()
+            em.append(e0.elapsed_time(e1))
+        et = float(np.mean(em))
+        if world > 1:
+            t = torch.tensor([et], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            et = float(t.item())
+        e2e = {"value": world * n / (et * 1e-3), "unit": "cells/s",
+               "h2d_bytes_per_step": int(n * (raw.n_eqns + 2) * 8),
+               "d2h_bytes_per_step": int(n * (raw.n_species + 1) * 8),
+               "api": "GpuKernelEvaluator.computeRR -> gf_compute_rr (pinned host arrays)"}
+        del ev
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r, done, kind, t = cpu_reference_rate(raw, cells, args.solver, wl["dT"], args.cpu_seconds, nthreads)
+        cpu = {"value": r, "unit": "cells/s", "cores": nthreads, "kind": kind,
+               "sample": f"first {done} cells of the {args.workload} batch ({t:.1f} s), the reference's "
+                         f"singleCellSolver per cell, OpenMP schedule(dynamic,64)"}
+
+    if rank == 0:
+        line = {
+            "metric": f"cells/s per ΔT at relTol 1e-4 ({args.workload}, R{args.solver}, persistent kernel)",
+            "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "cells_per_gpu": n, "species": raw.n_species,
+                       "reactions": raw.n_reactions, "deltaT": wl["dT"], "deltaTChem0": DTC0,
+                       "solver": f"Rosenbrock{args.solver}", "relTol": 1e-4, "absTol": 1e-8,
+                       "launch": solver.get_launch(), "l2": "inputs larger than L2 (not flushed)",
+                       "parallelism": f"cells sharded over {world} GPU(s)"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value, "traffic": None,
+                         "peak_source": "measured DFMA microbenchmark on this GPU (gf_measure_fp64_peak)",
+                         "algorithmic_flop_per_launch": flop, "attempts": attempts, "accepted": accepted},
+            "plain": plain,
+            "persistent_vs_plain": (value / plain["value"]) if plain else None,
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

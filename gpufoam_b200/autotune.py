@@ -1,0 +1,135 @@
+"""Launch-form autotuner of the chemistry kernels.
+
+For a mechanism and ODE settings it times every launch form the library
+offers on a sample of the caller's cells and keeps the fastest:
+
+  * plain: one thread per cell, HBM scratch (the reference's launch model);
+  * persistent work queue with G = 1, 2, 4, 8, 16, 32 threads per cell, the
+    per-cell workspace in shared memory (when it fits) or in HBM, and a range
+    of CTAs per SM.
+
+Results are cached per (device, mechanism shape, solver) in memory and in a
+JSON file (GPUFOAM_AUTOTUNE_CACHE, default ~/.cache/gpufoam_b200/autotune.json).
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import evaluator as E
+
+_CACHE: Dict[str, dict] = {}
+
+
+def _cache_path() -> str:
+    return os.environ.get("GPUFOAM_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "gpufoam_b200", "autotune.json"))
+
+
+def _key(mechs, ode: E.OdeInputs) -> str:
+    import torch
+    h = hashlib.sha1()
+    h.update(torch.cuda.get_device_name().encode())
+    for m in mechs:
+        h.update(f"{m.n_species}/{m.n_reactions}/{m.raw.name}".encode())
+    h.update(f"{ode.name}/{ode.relTol}/{ode.absTol}".encode())
+    return h.hexdigest()[:16]
+
+
+def candidates(max_ws_doubles: int) -> List[dict]:
+    fits = max_ws_doubles * 8 <= 227 * 1024
+    out = [dict(kind=0, threads_per_cell=1, scratch_in_shared=0, cells_per_block=0, blocks_per_sm=0,
+                register_budget=0)]
+    for G in (1, 4, 8, 16, 32):
+        for shared in ((1, 0) if fits else (0,)):
+            if shared and G == 1 and max_ws_doubles * 8 * 32 > 227 * 1024:
+                continue
+            for regs in (0, 1):
+                out.append(dict(kind=1, threads_per_cell=G, scratch_in_shared=shared, cells_per_block=0,
+                                blocks_per_sm=0, register_budget=regs))
+    return out
+
+
+def time_config(solver: E.Solver, cfg: dict, Y0, dtc0, deltaT: float, reps: int = 2, deltaT_cell=None,
+                mech_id=None) -> float:
+    """Mean ms of one solve over the sample with launch form cfg."""
+    import torch
+    solver.set_launch(**cfg)
+    dtc = dtc0.clone()
+    Ynew = torch.empty_like(Y0)
+    solver.solve(Y0, deltaT, dtc, Ynew=Ynew, deltaT_cell=deltaT_cell, mech_id=mech_id, want_status=False,
+                 want_counters=False, want_stats=False)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        dtc.copy_(dtc0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        solver.solve(Y0, deltaT, dtc, Ynew=Ynew, deltaT_cell=deltaT_cell, mech_id=mech_id, want_status=False,
+                     want_counters=False, want_stats=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return float(np.mean(ms))
+
+
+def tune(solver: E.Solver, Y_sample, deltaT: float, dtc0: float = 1e-7, deltaT_cell=None, mech_id=None,
+         configs: Optional[List[dict]] = None, use_cache: bool = True, verbose: bool = False) -> dict:
+    """Pick the fastest launch form for `solver` on a sample of cells and apply
+    it. Returns dict(best=cfg, table=[(cfg, ms)])."""
+    import torch
+    key = _key(solver.mechs, solver.ode)
+    if use_cache and key in _CACHE:
+        solver.set_launch(**_CACHE[key]["best"])
+        return _CACHE[key]
+    if use_cache and key not in _CACHE and os.path.exists(_cache_path()):
+        try:
+            disk = json.load(open(_cache_path()))
+            if key in disk:
+                _CACHE[key] = disk[key]
+                solver.set_launch(**disk[key]["best"])
+                return disk[key]
+        except Exception:
+            pass
+    Y0 = torch.as_tensor(Y_sample, dtype=torch.float64, device="cuda").contiguous()
+    d0 = torch.full((Y0.shape[0],), dtc0, dtype=torch.float64, device="cuda")
+    ws = max(_ws_doubles(m) for m in solver.mechs)
+    table = []
+    for cfg in configs or candidates(ws):
+        try:
+            ms = time_config(solver, cfg, Y0, d0, deltaT, deltaT_cell=deltaT_cell, mech_id=mech_id)
+        except Exception as e:  # a form the device cannot launch
+            if verbose:
+                print("skip", cfg, e)
+            continue
+        table.append((cfg, ms))
+        if verbose:
+            print(json.dumps(cfg), f"{ms:.2f} ms")
+    best = min(table, key=lambda t: t[1])[0]
+    solver.set_launch(**best)
+    res = dict(best=best, table=table)
+    _CACHE[key] = res
+    if use_cache:
+        try:
+            os.makedirs(os.path.dirname(_cache_path()), exist_ok=True)
+            disk = json.load(open(_cache_path())) if os.path.exists(_cache_path()) else {}
+            disk[key] = res
+            json.dump(disk, open(_cache_path(), "w"))
+        except Exception:
+            pass
+    return res
+
+
+def _ws_doubles(mech: E.Mechanism) -> int:
+    """Per-cell workspace in doubles (mirrors make_layout in gf_device.cuh)."""
+    nS = mech.n_species
+    m = nS + 1
+    ld = m | 1
+    slots = 0
+    for r in mech.raw.reactions:
+        slots += 2 + len(r.lhs) + len(r.rhs) + (2 if r.rate_type == 1 else 0)
+    return m * ld + 12 * m + 5 * nS + 3 * max(mech.n_reactions, 1) + max(slots, 1) + 8

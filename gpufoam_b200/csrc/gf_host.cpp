@@ -1,0 +1,705 @@
+// Host side of the C ABI (include/gpufoam_b200.h): mechanism loader arithmetic,
+// device mechanism tables, solver objects and the per-flow-step solve.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "gf_internal.h"
+
+namespace {
+
+// gpu_utils/common/gpu_constants.H:13-82
+constexpr double kRR = 6.02214e+26 * 1.38065e-23;
+constexpr double kSmall = DBL_EPSILON;
+constexpr double kVSmall = DBL_MIN;
+constexpr double kGreat = 1.0 / DBL_EPSILON;
+
+thread_local std::string g_last_cuda_error;
+
+int cuda_fail(cudaError_t e) {
+    g_last_cuda_error = cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return GF_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GF_ERR_NO_DEVICE;
+    return GF_ERR_CUDA;
+}
+
+#define GF_CUDA(x)                                  \
+    do {                                            \
+        cudaError_t e_ = (x);                       \
+        if (e_ != cudaSuccess) return cuda_fail(e_); \
+    } while (0)
+
+// ---- reference loader arithmetic on gf_thermo (gpuThermo.H:352-470,
+//      gpuPerfectGas.H:100-117, 280-325)
+
+void thermo_add(gf_thermo& a, const gf_thermo& b) {
+    double Y1 = a.Y;
+    const double sumY = a.Y + b.Y;
+    if (std::fabs(sumY) > kSmall) a.W = sumY / (a.Y / a.W + b.Y / b.W);
+    a.Y = sumY;
+    if (std::fabs(a.Y) > kSmall) {
+        Y1 /= a.Y;
+        const double Y2 = b.Y / a.Y;
+        a.Tlow = std::max(a.Tlow, b.Tlow);
+        a.Thigh = std::min(a.Thigh, b.Thigh);
+        for (int k = 0; k < 7; ++k) {
+            a.high[k] = Y1 * a.high[k] + Y2 * b.high[k];
+            a.low[k] = Y1 * a.low[k] + Y2 * b.low[k];
+        }
+    }
+}
+
+gf_thermo thermo_eq(const gf_thermo& t1, const gf_thermo& t2) {
+    gf_thermo r;
+    double diffY = t2.Y - t1.Y;
+    if (std::fabs(diffY) < kSmall) diffY = kSmall;
+    const double diffRW = t2.Y / t2.W - t1.Y / t1.W;
+    double molWeight = kGreat;
+    if (std::fabs(diffRW) > kSmall) molWeight = diffY / diffRW;
+    r.Y = diffY;
+    r.W = molWeight;
+    const double Y1 = t2.Y / r.Y;
+    const double Y2 = t1.Y / r.Y;
+    for (int k = 0; k < 7; ++k) {
+        r.high[k] = Y1 * t2.high[k] - Y2 * t1.high[k];
+        r.low[k] = Y1 * t2.low[k] - Y2 * t1.low[k];
+    }
+    r.Tlow = std::max(t2.Tlow, t1.Tlow);
+    r.Thigh = std::min(t2.Thigh, t1.Thigh);
+    r.Tcommon = t2.Tcommon;
+    return r;
+}
+
+gf_thermo thermo_scaled(const gf_thermo& t, double stoich) {
+    gf_thermo r = t;
+    r.Y = (stoich * t.W) * t.Y;
+    return r;
+}
+
+bool valid_ptr(const void* p) { return p != nullptr; }
+
+// ---- device buffer with sub-allocation
+
+struct DevBuf {
+    std::vector<char> host;
+    size_t add(const void* src, size_t bytes) {
+        const size_t off = (host.size() + 255) & ~size_t(255);
+        host.resize(off + bytes);
+        if (bytes) std::memcpy(host.data() + off, src, bytes);
+        return off;
+    }
+    template <class T>
+    size_t add(const std::vector<T>& v) {
+        return add(v.data(), v.size() * sizeof(T));
+    }
+};
+
+}  // namespace
+
+struct gf_mech {
+    gf::DevMech dev;
+    void* dmem = nullptr;
+    long long bytes = 0;
+    int device = 0;
+};
+
+struct gf_solver {
+    std::vector<const gf_mech*> mechs;
+    std::vector<gf::DevMech> dmechs;
+    gf::OdeParams ode;
+    double Treact = 0.0;
+    gf_launch_config cfg;
+    unsigned long long* queue = nullptr;  // device
+    unsigned long long* queue_host = nullptr;  // pinned
+    double* ws = nullptr;
+    size_t ws_bytes = 0;
+    int max_ws_doubles = 0;
+    int max_neq = 0;
+    // device staging for the host-memory entry points
+    double* dY = nullptr;
+    double* dYnew = nullptr;
+    double* dRR = nullptr;
+    double* drho = nullptr;
+    double* ddtc = nullptr;
+    int staged_cells = 0;
+};
+
+namespace {
+
+int ensure_ws(gf_solver* s, size_t bytes) {
+    if (bytes <= s->ws_bytes) return GF_OK;
+    if (s->ws) cudaFree(s->ws);
+    s->ws = nullptr;
+    s->ws_bytes = 0;
+    GF_CUDA(cudaMalloc(&s->ws, bytes));
+    s->ws_bytes = bytes;
+    return GF_OK;
+}
+
+int ensure_staging(gf_solver* s, int n) {
+    if (n <= s->staged_cells) return GF_OK;
+    cudaFree(s->dY);
+    cudaFree(s->dYnew);
+    cudaFree(s->dRR);
+    cudaFree(s->drho);
+    cudaFree(s->ddtc);
+    s->dY = s->dYnew = s->dRR = s->drho = s->ddtc = nullptr;
+    s->staged_cells = 0;
+    const size_t ne = (size_t)s->max_neq;
+    GF_CUDA(cudaMalloc(&s->dY, (size_t)n * ne * sizeof(double)));
+    GF_CUDA(cudaMalloc(&s->dYnew, (size_t)n * ne * sizeof(double)));
+    GF_CUDA(cudaMalloc(&s->dRR, (size_t)n * ne * sizeof(double)));
+    GF_CUDA(cudaMalloc(&s->drho, (size_t)n * sizeof(double)));
+    GF_CUDA(cudaMalloc(&s->ddtc, (size_t)n * sizeof(double)));
+    s->staged_cells = n;
+    return GF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf_abi_version(void) { return GF_ABI_VERSION; }
+
+const char* gf_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
+
+const char* gf_strerror(int status) {
+    switch (status) {
+    case GF_OK: return "ok";
+    case GF_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case GF_ERR_UNKNOWN_SOLVER: return "Invalid ODE Solver type";
+    case GF_ERR_UNSUPPORTED: return "mechanism outside the supported limits";
+    case GF_ERR_MASS_IMBALANCE: return "mass imbalance in reaction (> 0.1 kg/kmol)";
+    case GF_ERR_CUDA: return "CUDA runtime error";
+    case GF_ERR_NO_DEVICE: return "no CUDA device";
+    case GF_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case GF_ERR_CELL_FAILURE: return "one or more cells failed to integrate";
+    default: return "unknown status";
+    }
+}
+
+// makeGpuThermo (makeGpuThermo.H:16-48)
+int gf_thermo_from_nasa(double Y, double W, double Tlow, double Thigh, double Tcommon, const double high_raw[7],
+                        const double low_raw[7], gf_thermo* out) {
+    if (!high_raw || !low_raw || !out || !(W > 0)) return GF_ERR_INVALID_ARGUMENT;
+    const double R = kRR / W;  // specie gas constant, gpuPerfectGas.H:141-143
+    out->Y = Y;
+    out->W = W;
+    out->Tlow = Tlow;
+    out->Thigh = Thigh;
+    out->Tcommon = Tcommon;
+    for (int k = 0; k < 7; ++k) {
+        out->high[k] = R * high_raw[k];
+        out->low[k] = R * low_raw[k];
+    }
+    return GF_OK;
+}
+
+// set_reaction_thermo (makeGpuReactions.H:18-59)
+int gf_reaction_thermo(const gf_thermo* species, int n_species, int n_lhs, const gf_specie_coeff* lhs, int n_rhs,
+                       const gf_specie_coeff* rhs, gf_thermo* out) {
+    if (!species || !lhs || !rhs || !out || n_lhs < 1 || n_rhs < 1) return GF_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n_lhs; ++i)
+        if (lhs[i].index < 0 || lhs[i].index >= n_species) return GF_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n_rhs; ++i)
+        if (rhs[i].index < 0 || rhs[i].index >= n_species) return GF_ERR_INVALID_ARGUMENT;
+    gf_thermo r = thermo_scaled(species[rhs[0].index], rhs[0].stoich);
+    for (int i = 1; i < n_rhs; ++i) thermo_add(r, thermo_scaled(species[rhs[i].index], rhs[i].stoich));
+    gf_thermo l = thermo_scaled(species[lhs[0].index], lhs[0].stoich);
+    for (int i = 1; i < n_lhs; ++i) thermo_add(l, thermo_scaled(species[lhs[i].index], lhs[i].stoich));
+    if (std::fabs(l.Y - r.Y) > 0.1) return GF_ERR_MASS_IMBALANCE;
+    *out = thermo_eq(l, r);
+    return GF_OK;
+}
+
+int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
+    if (!d || !out || !d->thermos || (d->n_reactions > 0 && !d->reactions)) return GF_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    const int nS = d->n_species, nR = d->n_reactions;
+    if (nS < 1 || nR < 0) return GF_ERR_INVALID_ARGUMENT;
+    if (nS > GF_MAX_SPECIES) return GF_ERR_UNSUPPORTED;
+    using namespace gf;
+    // ---- validation
+    double Tlow = 0, Thigh = DBL_MAX / 10;
+    if (!(nR >= 0)) return GF_ERR_INVALID_ARGUMENT;
+    for (int r = 0; r < nR; ++r) {
+        const gf_reaction& x = d->reactions[r];
+        if (x.n_lhs < 1 || x.n_rhs < 1 || x.n_lhs > kMaxW || x.n_rhs > kMaxW) return GF_ERR_UNSUPPORTED;
+        if (x.rate_type < 0 || x.rate_type > 3) return GF_ERR_INVALID_ARGUMENT;
+        if (x.rate_type != GF_RATE_ARRHENIUS && !x.efficiencies) return GF_ERR_INVALID_ARGUMENT;
+        for (int i = 0; i < x.n_lhs; ++i)
+            if (x.lhs[i].index < 0 || x.lhs[i].index >= nS) return GF_ERR_INVALID_ARGUMENT;
+        for (int i = 0; i < x.n_rhs; ++i)
+            if (x.rhs[i].index < 0 || x.rhs[i].index >= nS) return GF_ERR_INVALID_ARGUMENT;
+        // one set of limits per mechanism, as makeGpuReactions sets them (makeGpuReactions.H:121-124)
+        if (r == 0) {
+            Tlow = x.Tlow;
+            Thigh = x.Thigh;
+        } else if (x.Tlow != Tlow || x.Thigh != Thigh) {
+            return GF_ERR_UNSUPPORTED;
+        }
+    }
+    for (int i = 0; i < nS; ++i)
+        if (!(d->thermos[i].W > 0)) return GF_ERR_INVALID_ARGUMENT;
+
+    // ---- host tables
+    std::vector<double> W(nS), Rsp(nS), Tc(nS), coef((size_t)14 * nS);
+    for (int i = 0; i < nS; ++i) {
+        const gf_thermo& t = d->thermos[i];
+        W[i] = t.W;
+        Rsp[i] = kRR / t.W;
+        Tc[i] = t.Tcommon;
+        for (int k = 0; k < 7; ++k) {
+            coef[(size_t)k * nS + i] = t.low[k];
+            coef[(size_t)(7 + k) * nS + i] = t.high[k];
+        }
+    }
+    const int nRa = std::max(nR, 1);
+    // compute order: reactions grouped by rate type (stable within a type)
+    std::vector<int> qof(nRa, 0), rof(nRa, 0);  // q -> r and r -> q
+    {
+        std::vector<int> o(nR);
+        for (int r = 0; r < nR; ++r) o[r] = r;
+        std::stable_sort(o.begin(), o.end(),
+                         [&](int a, int b) { return d->reactions[a].rate_type < d->reactions[b].rate_type; });
+        for (int q = 0; q < nR; ++q) {
+            qof[q] = o[q];
+            rof[o[q]] = q;
+        }
+    }
+    std::vector<int> rtype(nRa), rirr(nRa), nl(nRa), nr(nRa), sp_off(nRa + 1, 0), slot(nRa + 1, 0),
+        rnm_small(nRa), tb_row(nRa, -1);
+    std::vector<double> rY(nRa), rnm(nRa), rTc(nRa), rcoef((size_t)14 * nRa), troe((size_t)4 * nRa, 0.0);
+    std::vector<double> lnA0(nRa), sA0(nRa), beta0(nRa), Ta0(nRa), lnA1(nRa, 0.0), sA1(nRa, 0.0), beta1(nRa, 0.0),
+        Ta1(nRa, 0.0);
+    std::vector<int> sidx, siexp;
+    std::vector<double> sst, sexp, eff;
+    auto logabs = [](double A, double* lnA, double* sA) {
+        // k = sign(A) exp(ln|A| + ...): A == 0 gives sign 0 (k == 0 exactly)
+        *sA = A > 0 ? 1.0 : (A < 0 ? -1.0 : 0.0);
+        *lnA = A != 0 ? std::log(std::fabs(A)) : 0.0;
+    };
+    int n_tb = 0;
+    for (int q = 0; q < nR; ++q) {
+        const gf_reaction& x = d->reactions[qof[q]];
+        rtype[q] = x.rate_type;
+        rirr[q] = x.irreversible ? 1 : 0;
+        nl[q] = x.n_lhs;
+        nr[q] = x.n_rhs;
+        rY[q] = x.thermo.Y;
+        const double nm = x.thermo.Y / x.thermo.W;
+        rnm[q] = nm;
+        rnm_small[q] = std::fabs(nm - kSmall) < kVSmall ? 1 : 0;  // gpuThermo.H:111, 146
+        rTc[q] = x.thermo.Tcommon;
+        for (int k = 0; k < 7; ++k) {
+            rcoef[(size_t)k * nRa + q] = x.thermo.low[k];
+            rcoef[(size_t)(7 + k) * nRa + q] = x.thermo.high[k];
+        }
+        logabs(x.A, &lnA0[q], &sA0[q]);
+        beta0[q] = x.beta;
+        Ta0[q] = x.Ta;
+        if (x.rate_type == GF_RATE_LINDEMANN_FALLOFF || x.rate_type == GF_RATE_TROE_FALLOFF) {
+            logabs(x.Ainf, &lnA1[q], &sA1[q]);
+            beta1[q] = x.betainf;
+            Ta1[q] = x.Tainf;
+        }
+        troe[4 * q + 0] = x.troe_alpha;
+        troe[4 * q + 1] = 1.0 / x.troe_Tsss;
+        troe[4 * q + 2] = 1.0 / x.troe_Ts;
+        troe[4 * q + 3] = x.troe_Tss;
+        if (x.rate_type != GF_RATE_ARRHENIUS) {
+            tb_row[q] = n_tb++;
+            eff.insert(eff.end(), x.efficiencies, x.efficiencies + nS);
+        }
+        for (int e = 0; e < x.n_lhs + x.n_rhs; ++e) {
+            const gf_specie_coeff& sc = e < x.n_lhs ? x.lhs[e] : x.rhs[e - x.n_lhs];
+            sidx.push_back(sc.index);
+            sst.push_back(sc.stoich);
+            if (sc.integer_exponent) {
+                siexp.push_back((int)sc.exponent);
+                sexp.push_back((double)(int)sc.exponent);
+            } else {
+                siexp.push_back(kNoIntExp);
+                sexp.push_back(sc.exponent);
+            }
+        }
+        sp_off[q + 1] = sp_off[q] + x.n_lhs + x.n_rhs;
+        slot[q + 1] = slot[q] + 2 + x.n_lhs + x.n_rhs + (x.rate_type == GF_RATE_THIRD_BODY_ARRHENIUS ? 2 : 0);
+    }
+    const int n_slots = slot[nR];
+    // per-species terms, built over reactions in mechanism order r
+    std::vector<std::vector<std::pair<int, double>>> dn(nS);
+    std::vector<std::vector<JrRec>> jr(nS);
+    std::vector<int> tbt_q, tbt_s;
+    std::vector<double> tbt_coef;
+    for (int r = 0; r < nR; ++r) {
+        const gf_reaction& x = d->reactions[r];
+        const int so = slot[rof[r]];
+        // dNdtByV (gpuReaction.H:490-508)
+        for (int i = 0; i < x.n_lhs; ++i) dn[x.lhs[i].index].push_back({so, -x.lhs[i].stoich});
+        for (int i = 0; i < x.n_rhs; ++i) dn[x.rhs[i].index].push_back({so, x.rhs[i].stoich});
+        auto add = [&](int s, int c, int sl, double cf) { jr[s].push_back(JrRec{c, sl, cf}); };
+        // jac_dCfdcj_contribution (gpuReaction.H:547-569)
+        for (int j = 0; j < x.n_lhs; ++j) {
+            const int sj = x.lhs[j].index;
+            for (int i = 0; i < x.n_lhs; ++i) add(x.lhs[i].index, sj, so + 2 + j, -x.lhs[i].stoich);
+            for (int i = 0; i < x.n_rhs; ++i) add(x.rhs[i].index, sj, so + 2 + j, x.rhs[i].stoich);
+        }
+        // jac_dCrdcj_contribution (:571-593); an irreversible reaction adds zeros
+        if (!x.irreversible) {
+            for (int j = 0; j < x.n_rhs; ++j) {
+                const int sj = x.rhs[j].index;
+                for (int i = 0; i < x.n_lhs; ++i) add(x.lhs[i].index, sj, so + 2 + x.n_lhs + j, x.lhs[i].stoich);
+                for (int i = 0; i < x.n_rhs; ++i) add(x.rhs[i].index, sj, so + 2 + x.n_lhs + j, -x.rhs[i].stoich);
+            }
+        }
+        // jac_dCdT_contribution (:595-612)
+        for (int i = 0; i < x.n_lhs; ++i) add(x.lhs[i].index, nS, so + 1, -x.lhs[i].stoich);
+        for (int i = 0; i < x.n_rhs; ++i) add(x.rhs[i].index, nS, so + 1, x.rhs[i].stoich);
+        // jac_dCdC_contribution (:614-648): fall-off ddc is identically zero (kInf
+        // has no concentration dependence, gpuFallOffReactionRate.H:143-153)
+        if (x.rate_type == GF_RATE_THIRD_BODY_ARRHENIUS) {
+            for (int i = 0; i < x.n_lhs; ++i) {
+                tbt_q.push_back(rof[r]);
+                tbt_s.push_back(x.lhs[i].index);
+                tbt_coef.push_back(-x.lhs[i].stoich);
+            }
+            for (int i = 0; i < x.n_rhs; ++i) {
+                tbt_q.push_back(rof[r]);
+                tbt_s.push_back(x.rhs[i].index);
+                tbt_coef.push_back(x.rhs[i].stoich);
+            }
+        }
+    }
+    std::vector<int> dn_ptr(nS + 1, 0), dn_slot;
+    std::vector<double> dn_coef;
+    std::vector<int> jr_ptr(nS + 1, 0);
+    std::vector<JrRec> jr_all;
+    for (int s = 0; s < nS; ++s) {
+        for (auto& t : dn[s]) {
+            dn_slot.push_back(t.first);
+            dn_coef.push_back(t.second);
+        }
+        dn_ptr[s + 1] = (int)dn_slot.size();
+        jr_all.insert(jr_all.end(), jr[s].begin(), jr[s].end());
+        jr_ptr[s + 1] = (int)jr_all.size();
+    }
+    const int n_tbt = (int)tbt_q.size();
+    std::vector<double> eff_t((size_t)nS * std::max(n_tb, 1), 0.0);
+    for (int t = 0; t < n_tb; ++t)
+        for (int i = 0; i < nS; ++i) eff_t[(size_t)i * n_tb + t] = eff[(size_t)t * nS + i];
+    // keep every array non-empty
+    if (eff.empty()) eff.push_back(0.0);
+    if (sidx.empty()) {
+        sidx.push_back(0);
+        siexp.push_back(0);
+        sst.push_back(0.0);
+        sexp.push_back(0.0);
+    }
+    if (dn_slot.empty()) {
+        dn_slot.push_back(0);
+        dn_coef.push_back(0.0);
+    }
+    if (jr_all.empty()) jr_all.push_back(JrRec{0, 0, 0.0});
+    if (tbt_q.empty()) {
+        tbt_q.push_back(0);
+        tbt_s.push_back(0);
+        tbt_coef.push_back(0.0);
+    }
+
+    // ---- one device allocation
+    DevBuf b;
+    const size_t oW = b.add(W), oR = b.add(Rsp), oTc = b.add(Tc), oCoef = b.add(coef);
+    const size_t oRt = b.add(rtype), oRi = b.add(rirr), oNl = b.add(nl), oNr = b.add(nr), oSpo = b.add(sp_off),
+                 oSlot = b.add(slot), oRY = b.add(rY), oRnm = b.add(rnm), oRns = b.add(rnm_small), oRTc = b.add(rTc),
+                 oRc = b.add(rcoef), oLA0 = b.add(lnA0), oSA0 = b.add(sA0), oB0 = b.add(beta0), oT0 = b.add(Ta0),
+                 oLA1 = b.add(lnA1), oSA1 = b.add(sA1), oB1 = b.add(beta1), oT1 = b.add(Ta1), oTroe = b.add(troe),
+                 oTb = b.add(tb_row), oEff = b.add(eff), oEffT = b.add(eff_t), oSi = b.add(sidx), oSie = b.add(siexp), oSst = b.add(sst),
+                 oSe = b.add(sexp), oDnp = b.add(dn_ptr), oDns = b.add(dn_slot), oDnc = b.add(dn_coef),
+                 oJrp = b.add(jr_ptr), oJr = b.add(jr_all), oTbq = b.add(tbt_q), oTbs = b.add(tbt_s),
+                 oTbc = b.add(tbt_coef);
+    gf_mech* m = new (std::nothrow) gf_mech;
+    if (!m) return GF_ERR_OUT_OF_MEMORY;
+    cudaGetDevice(&m->device);
+    cudaError_t e = cudaMalloc(&m->dmem, b.host.size());
+    if (e != cudaSuccess) {
+        delete m;
+        return cuda_fail(e);
+    }
+    e = cudaMemcpy(m->dmem, b.host.data(), b.host.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(m->dmem);
+        delete m;
+        return cuda_fail(e);
+    }
+    m->bytes = (long long)b.host.size();
+    char* base = static_cast<char*>(m->dmem);
+    auto P = [&](size_t o) { return base + o; };
+    DevMech& D = m->dev;
+    D.nS = nS;
+    D.nR = nR;
+    D.m = nS + 1;
+    D.n_slots = n_slots;
+    D.n_tb = n_tb;
+    D.n_tbt = n_tbt;
+    D.Tlow = Tlow;
+    D.Thigh = Thigh;
+    D.W = (const double*)P(oW);
+    D.Rsp = (const double*)P(oR);
+    D.Tcommon = (const double*)P(oTc);
+    D.coef = (const double*)P(oCoef);
+    D.rtype = (const int*)P(oRt);
+    D.rirr = (const int*)P(oRi);
+    D.nl = (const int*)P(oNl);
+    D.nr = (const int*)P(oNr);
+    D.sp_off = (const int*)P(oSpo);
+    D.slot = (const int*)P(oSlot);
+    D.rY = (const double*)P(oRY);
+    D.rnm = (const double*)P(oRnm);
+    D.rnm_small = (const int*)P(oRns);
+    D.rTcommon = (const double*)P(oRTc);
+    D.rcoef = (const double*)P(oRc);
+    D.lnA0 = (const double*)P(oLA0);
+    D.sA0 = (const double*)P(oSA0);
+    D.beta0 = (const double*)P(oB0);
+    D.Ta0 = (const double*)P(oT0);
+    D.lnA1 = (const double*)P(oLA1);
+    D.sA1 = (const double*)P(oSA1);
+    D.beta1 = (const double*)P(oB1);
+    D.Ta1 = (const double*)P(oT1);
+    D.troe = (const double*)P(oTroe);
+    D.tb_row = (const int*)P(oTb);
+    D.eff = (const double*)P(oEff);
+    D.eff_t = (const double*)P(oEffT);
+    D.sidx = (const int*)P(oSi);
+    D.siexp = (const int*)P(oSie);
+    D.sst = (const double*)P(oSst);
+    D.sexp = (const double*)P(oSe);
+    D.dn_ptr = (const int*)P(oDnp);
+    D.dn_slot = (const int*)P(oDns);
+    D.dn_coef = (const double*)P(oDnc);
+    D.jr_ptr = (const int*)P(oJrp);
+    D.jr = (const JrRec*)P(oJr);
+    D.tbt_q = (const int*)P(oTbq);
+    D.tbt_s = (const int*)P(oTbs);
+    D.tbt_coef = (const double*)P(oTbc);
+    *out = m;
+    return GF_OK;
+}
+
+void gf_mech_destroy(gf_mech* m) {
+    if (!m) return;
+    if (m->dmem) cudaFree(m->dmem);
+    delete m;
+}
+
+int gf_mech_info(const gf_mech* m, int* n_species, int* n_reactions, long long* device_bytes) {
+    if (!m) return GF_ERR_INVALID_ARGUMENT;
+    if (n_species) *n_species = m->dev.nS;
+    if (n_reactions) *n_reactions = m->dev.nR;
+    if (device_bytes) *device_bytes = m->bytes;
+    return GF_OK;
+}
+
+int gf_solver_create(const gf_mech* const* mechs, int n_mechs, const gf_ode_inputs* in, double Treact,
+                     gf_solver** out) {
+    if (!mechs || n_mechs < 1 || n_mechs > 4 || !in || !out) return GF_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    // make_gpuODESolver (makeGpuOdeSolver.H:13-31)
+    if (in->solver != GF_ROSENBROCK12 && in->solver != GF_ROSENBROCK23 && in->solver != GF_ROSENBROCK34)
+        return GF_ERR_UNKNOWN_SOLVER;
+    if (in->maxSteps < 0) return GF_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n_mechs; ++i)
+        if (!mechs[i]) return GF_ERR_INVALID_ARGUMENT;
+    gf_solver* s = new (std::nothrow) gf_solver;
+    if (!s) return GF_ERR_OUT_OF_MEMORY;
+    for (int i = 0; i < n_mechs; ++i) {
+        s->mechs.push_back(mechs[i]);
+        s->dmechs.push_back(mechs[i]->dev);
+        s->max_ws_doubles = std::max(s->max_ws_doubles, gf::ws_layout(mechs[i]->dev).size);
+        s->max_neq = std::max(s->max_neq, mechs[i]->dev.nS + 2);
+    }
+    s->ode = gf::OdeParams{in->solver, in->absTol, in->relTol, in->maxSteps, in->safeScale, in->alphaInc,
+                           in->alphaDec, in->minScale, in->maxScale};
+    s->Treact = Treact;
+    // default launch: persistent, a warp per cell, workspace in shared memory
+    // when it fits (the autotuner refines this per mechanism)
+    s->cfg = gf_launch_config{1, 32, 1, 1, 0, 0};  // kind, G, shared, cells/CTA, CTAs/SM, registers
+    if ((size_t)s->max_ws_doubles * sizeof(double) > 227 * 1024) s->cfg.scratch_in_shared = 0;
+    cudaError_t e = cudaMalloc(&s->queue, 8 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->queue_host, 8 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        gf_solver_destroy(s);
+        return cuda_fail(e);
+    }
+    *out = s;
+    return GF_OK;
+}
+
+void gf_solver_destroy(gf_solver* s) {
+    if (!s) return;
+    cudaFree(s->queue);
+    if (s->queue_host) cudaFreeHost(s->queue_host);
+    cudaFree(s->ws);
+    cudaFree(s->dY);
+    cudaFree(s->dYnew);
+    cudaFree(s->dRR);
+    cudaFree(s->drho);
+    cudaFree(s->ddtc);
+    delete s;
+}
+
+int gf_solver_set_launch(gf_solver* s, const gf_launch_config* cfg) {
+    if (!s || !cfg) return GF_ERR_INVALID_ARGUMENT;
+    if (cfg->kind != 0 && cfg->kind != 1) return GF_ERR_INVALID_ARGUMENT;
+    if (cfg->kind == 1) {
+        const int G = cfg->threads_per_cell;
+        if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) return GF_ERR_INVALID_ARGUMENT;
+        if (cfg->register_budget != 0 && cfg->register_budget != 1) return GF_ERR_INVALID_ARGUMENT;
+        if (cfg->scratch_in_shared && (size_t)s->max_ws_doubles * sizeof(double) > 227 * 1024)
+            return GF_ERR_UNSUPPORTED;
+    }
+    s->cfg = *cfg;
+    return GF_OK;
+}
+
+int gf_solver_get_launch(const gf_solver* s, gf_launch_config* cfg) {
+    if (!s || !cfg) return GF_ERR_INVALID_ARGUMENT;
+    *cfg = s->cfg;
+    return GF_OK;
+}
+
+int gf_solve(gf_solver* s, int n_cells, double deltaT, const double* deltaT_cell, double deltaTChemMax,
+             const int* mech_id, const double* rho, const double* Y0, int ld_y, double* Ynew, double* deltaTChem,
+             double* RR, int ld_rr, int* status, int* counters, gf_stats* stats, void* stream) {
+    if (!s || n_cells < 0 || !deltaTChem || !Y0) return GF_ERR_INVALID_ARGUMENT;
+    if (ld_y < s->max_neq) return GF_ERR_INVALID_ARGUMENT;
+    if (RR && (!rho || ld_rr < 1)) return GF_ERR_INVALID_ARGUMENT;
+    if (!mech_id && s->mechs.size() > 1) return GF_ERR_INVALID_ARGUMENT;
+    if (RR && s->mechs.size() == 1 && ld_rr < s->dmechs[0].nS) return GF_ERR_INVALID_ARGUMENT;
+    gf::LaunchArgs a;
+    a.n_cells = n_cells;
+    a.deltaT = deltaT;
+    a.deltaT_cell = deltaT_cell;
+    a.deltaTChemMax = deltaTChemMax;
+    a.mech_id = mech_id;
+    a.rho = rho;
+    a.Y0 = Y0;
+    a.ld_y = ld_y;
+    a.Ynew = Ynew;
+    a.deltaTChem = deltaTChem;
+    a.RR = RR;
+    a.ld_rr = ld_rr;
+    a.status = status;
+    a.counters = counters;
+    a.Treact = s->Treact;
+    a.ode = s->ode;
+    a.queue = s->queue;
+    a.ws = nullptr;
+    a.ws_slot_stride = 0;
+    const int wsd = s->max_ws_doubles;
+    int slots = 0;
+    if (s->cfg.kind == 0) {
+        slots = n_cells;
+        a.ws_slot_stride = n_cells;
+    } else {
+        int blocks = 0, threads = 0;
+        slots = gf::persistent_slots(s->cfg, wsd * (int)sizeof(double), &blocks, &threads);
+        if (slots <= 0) return GF_ERR_UNSUPPORTED;
+        if (s->cfg.scratch_in_shared) slots = 0;
+    }
+    if (slots > 0) {
+        const int r = ensure_ws(s, (size_t)slots * wsd * sizeof(double));
+        if (r) return r;
+    }
+    a.ws = s->ws;
+    const int ce = gf::launch_cells(s->dmechs.data(), (int)s->dmechs.size(), s->cfg, a, wsd, slots, stream);
+    if (ce) return cuda_fail((cudaError_t)ce);
+    if (stats) {
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        GF_CUDA(cudaMemcpyAsync(s->queue_host, s->queue, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        const unsigned long long k = s->queue_host[1];
+        const unsigned long long bits = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+        double mn;
+        std::memcpy(&mn, &bits, 8);
+        stats->min_delta_t = n_cells > 0 ? mn : 0.0;
+        stats->accepted_steps = (long long)s->queue_host[2];
+        stats->attempts = (long long)s->queue_host[3];
+        stats->failed_cells = (long long)s->queue_host[4];
+    }
+    return GF_OK;
+}
+
+static int host_solve(gf_solver* s, int n, double deltaT, double deltaTChemMax, const double* rho,
+                      const double* deltaTChem, const double* Y, double* Ynew_out, double* RR_out,
+                      double* deltaTChemNew, double* minDeltaT) {
+    if (!s || n < 0 || !deltaTChem || !Y || !deltaTChemNew || s->mechs.size() != 1) return GF_ERR_INVALID_ARGUMENT;
+    if (n == 0) return GF_OK;
+    int r = ensure_staging(s, n);
+    if (r) return r;
+    const int ne = s->dmechs[0].nS + 2, nS = s->dmechs[0].nS;
+    GF_CUDA(cudaMemcpyAsync(s->dY, Y, (size_t)n * ne * sizeof(double), cudaMemcpyHostToDevice, 0));
+    GF_CUDA(cudaMemcpyAsync(s->ddtc, deltaTChem, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, 0));
+    if (RR_out) GF_CUDA(cudaMemcpyAsync(s->drho, rho, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, 0));
+    gf_stats st;
+    r = gf_solve(s, n, deltaT, nullptr, deltaTChemMax, nullptr, RR_out ? s->drho : nullptr, s->dY, ne, s->dYnew,
+                 s->ddtc, RR_out ? s->dRR : nullptr, nS, nullptr, nullptr, &st, 0);
+    if (r) return r;
+    if (Ynew_out) GF_CUDA(cudaMemcpy(Ynew_out, s->dYnew, (size_t)n * ne * sizeof(double), cudaMemcpyDeviceToHost));
+    if (RR_out) GF_CUDA(cudaMemcpy(RR_out, s->dRR, (size_t)n * nS * sizeof(double), cudaMemcpyDeviceToHost));
+    GF_CUDA(cudaMemcpy(deltaTChemNew, s->ddtc, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (minDeltaT) *minDeltaT = st.min_delta_t;
+    return GF_OK;
+}
+
+// GpuKernelEvaluator::computeRR (gpuKernelEvaluator.cu:65-97)
+int gf_compute_rr(gf_solver* s, int n, double deltaT, double deltaTChemMax, const double* rho,
+                  const double* deltaTChem, const double* Y, double* RR, double* deltaTChemNew, double* minDeltaT) {
+    if (!rho || !RR) return GF_ERR_INVALID_ARGUMENT;
+    return host_solve(s, n, deltaT, deltaTChemMax, rho, deltaTChem, Y, nullptr, RR, deltaTChemNew, minDeltaT);
+}
+
+// GpuKernelEvaluator::computeYNew (gpuKernelEvaluator.cu:35-63): deltaTChemNew unclamped
+int gf_compute_ynew(gf_solver* s, int n, double deltaT, double deltaTChemMax, const double* deltaTChem,
+                    const double* Y, double* Ynew, double* deltaTChemNew) {
+    (void)deltaTChemMax;
+    if (!Ynew) return GF_ERR_INVALID_ARGUMENT;
+    return host_solve(s, n, deltaT, INFINITY, nullptr, deltaTChem, Y, Ynew, nullptr, deltaTChemNew, nullptr);
+}
+
+int gf_rates(const gf_mech* m, int n, const double* y, double* dydx, void* stream) {
+    if (!m || n < 0 || (n > 0 && (!y || !dydx))) return GF_ERR_INVALID_ARGUMENT;
+    if ((size_t)gf::ws_layout(m->dev).size * sizeof(double) > 227 * 1024) return GF_ERR_UNSUPPORTED;
+    const int e = gf::launch_rates(m->dev, n, y, dydx, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
+}
+
+int gf_jacobian(const gf_mech* m, int n, const double* y, double* dfdx, double* J, void* stream) {
+    if (!m || n < 0 || (n > 0 && (!y || !dfdx || !J))) return GF_ERR_INVALID_ARGUMENT;
+    if ((size_t)gf::ws_layout(m->dev).size * sizeof(double) > 227 * 1024) return GF_ERR_UNSUPPORTED;
+    const int e = gf::launch_jacobian(m->dev, n, y, dfdx, J, nullptr, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
+}
+
+int gf_lu_decompose(int n_mats, int m, double* A, int* pivots, void* stream) {
+    if (n_mats < 0 || m < 1 || m > 160 || (n_mats > 0 && (!A || !pivots))) return GF_ERR_INVALID_ARGUMENT;
+    const int e = gf::launch_lu(n_mats, m, A, pivots, nullptr, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
+}
+
+int gf_lu_backsubstitute(int n_mats, int m, const double* LU, const int* pivots, double* b, void* stream) {
+    if (n_mats < 0 || m < 1 || m > 160 || (n_mats > 0 && (!LU || !pivots || !b))) return GF_ERR_INVALID_ARGUMENT;
+    const int e = gf::launch_lusolve(n_mats, m, LU, pivots, b, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
+}
+
+}  // extern "C"

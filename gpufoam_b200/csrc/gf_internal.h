@@ -1,0 +1,149 @@
+// Internal declarations shared by the host code (gf_host.cpp) and the CUDA
+// kernels (gf_kernels.cu). Not part of the public C ABI.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/gpufoam_b200.h"
+
+namespace gf {
+
+constexpr int kMaxW = GF_MAX_REACTION_WIDTH;
+constexpr int kNoIntExp = 2147483647 / 10;  // gpuLabelMax: "not an integer exponent"
+
+// One raw-Jacobian contribution of a species row: J[row][col] += coef * stage[slot].
+struct __align__(16) JrRec {
+    int col;
+    int slot;
+    double coef;
+};
+
+// Device-resident mechanism tables. All arrays are device pointers; the struct
+// itself is passed to kernels by value.
+//
+// Layout (nS species, nR reactions, m = nS + 1 unknowns of the linear
+// algebra: the pressure row and column of the reference Jacobian are
+// identically zero, gpuODESystem.H:101 and :195, so the solve runs on Y and T):
+//  * species NASA-7 coefficients: coef[(b * 7 + k) * nS + i], b = 0 low / 1 high
+//  * reactions are stored in "compute order" q (grouped by rate type, so that
+//    the lanes of a warp evaluate reactions of one kind together and read
+//    consecutive table entries); rcoef[(b * 7 + k) * nR + q] is the reaction
+//    ΔThermo. Arrhenius factors are kept as ln|A| and sign(A) (log-space
+//    evaluation k = sign * exp(ln|A| + beta ln T - Ta / T)); index 0 is k (or the
+//    fall-off k0), index 1 the fall-off kInf.
+//  * stoichiometry: compact CSR, sp_off[q] .. + nl[q] (lhs) + nr[q] (rhs)
+//  * staging slots of reaction q start at slot[q]:
+//      [0] omega, [1] dwdT, [2 .. 2+nl) dCf*kf, [2+nl .. 2+nl+nr) dCr*kr,
+//      third body only: [2+nl+nr] Ak, [3+nl+nr] (Cf - Cr/Kc)
+//  * dn_*: per species s, the (omega slot, signed stoich) terms of dN_s/dt in
+//    mechanism order (gpuReaction.H:490-508)
+//  * jr_*: per species row, the raw dN/dc and T-column contributions in the
+//    reference's update order (gpuReaction.H:547-612 over reactions in
+//    mechanism order)
+//  * tbt_*: the third-body dk/dc rows (gpuReaction.H:614-648): reaction q,
+//    species row s, signed stoich; row s gains coef * (eff[c] * Ak) * (Cf - Cr/Kc)
+//    in every species column c.
+struct DevMech {
+    int nS, nR, m;
+    int n_slots;
+    int n_tb;
+    int n_tbt;
+    double Tlow, Thigh;        // reaction temperature limits (uniform)
+    // species
+    const double* W;
+    const double* Rsp;         // RR / W
+    const double* Tcommon;
+    const double* coef;
+    // reactions, compute order
+    const int* rtype;
+    const int* rirr;
+    const int* nl;
+    const int* nr;
+    const int* sp_off;
+    const int* slot;
+    const double* rY;          // ΔThermo Y
+    const double* rnm;         // Y / W
+    const int* rnm_small;      // Kc = K when nm is "small" (gpuThermo.H:111)
+    const double* rTcommon;
+    const double* rcoef;
+    const double* lnA0;
+    const double* sA0;
+    const double* beta0;
+    const double* Ta0;
+    const double* lnA1;
+    const double* sA1;
+    const double* beta1;
+    const double* Ta1;
+    const double* troe;        // [nR][4]: alpha, 1/Tsss, 1/Ts, Tss
+    const int* tb_row;         // [nR] row of eff, -1 for plain Arrhenius
+    const double* eff;         // [n_tb][nS]
+    const double* eff_t;       // [nS][n_tb] (species-major: coalesced across reactions)
+    const int* sidx;
+    const int* siexp;          // integer exponent or kNoIntExp
+    const double* sst;
+    const double* sexp;
+    const int* dn_ptr;         // [nS + 1]
+    const int* dn_slot;
+    const double* dn_coef;
+    const int* jr_ptr;         // [nS + 1]
+    const JrRec* jr;
+    const int* tbt_q;
+    const int* tbt_s;
+    const double* tbt_coef;
+};
+
+struct OdeParams {
+    int solver;
+    double absTol, relTol;
+    int maxSteps;
+    double safeScale, alphaInc, alphaDec, minScale, maxScale;
+};
+
+// Per-cell workspace layout (in doubles) for a mechanism.
+struct WsLayout {
+    int ld;          // Jacobian / LU row stride (odd, bank-conflict free columns)
+    int J, y0, yt, dydx0, dydx, dfdx, k1, k2, k3, k4, c, Cp, Ha, rhoMbyW, vj, vv, piv, perm, kcache, stage, scal;
+    int size;        // total doubles
+};
+
+WsLayout ws_layout(const DevMech& m);
+
+struct LaunchArgs {
+    int n_cells;
+    double deltaT;
+    const double* deltaT_cell;
+    double deltaTChemMax;
+    const int* mech_id;
+    const double* rho;
+    const double* Y0;
+    int ld_y;
+    double* Ynew;
+    double* deltaTChem;
+    double* RR;
+    int ld_rr;
+    int* status;
+    int* counters;
+    double Treact;
+    OdeParams ode;
+    // device-side scratch owned by the solver
+    double* ws;                    // workspaces
+    long long ws_slot_stride;      // doubles per slot (blocked) or number of slots (interleaved)
+    unsigned long long* queue;     // [0] next cell, [1] min deltaTChem bits, [2] accepted, [3] attempts, [4] failed
+};
+
+// Kernel launchers (gf_kernels.cu). All return a cudaError_t as int.
+int launch_cells(const DevMech* mechs, int n_mechs, const gf_launch_config& cfg, const LaunchArgs& a,
+                 int ws_doubles_per_cell, int n_slots_total, void* stream);
+int launch_rates(const DevMech& m, int n, const double* y, double* dydx, void* stream);
+int launch_jacobian(const DevMech& m, int n, const double* y, double* dfdx, double* J, double* ws,
+                    void* stream);
+int launch_lu(int n_mats, int m, double* A, int* piv, double* vv, void* stream);
+int launch_lusolve(int n_mats, int m, const double* LU, const int* piv, double* b, void* stream);
+int launch_epilogue_reset(unsigned long long* queue, void* stream);
+
+// Resident-slot count for a persistent configuration (groups that run at once).
+int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* blocks_out, int* threads_out);
+int device_sm_count();
+
+}  // namespace gf

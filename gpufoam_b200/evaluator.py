@@ -1,0 +1,324 @@
+"""Host-side mirror of gpuFoam's chemistry evaluator, over the C ABI.
+
+Reference interfaces mirrored (paths relative to gpu_chemistry/src/):
+  * ``read_gpuODESolverInputs`` — gpuOde/readGpuOdeInputs.H:8-26 (defaults);
+  * ``make_gpu_thermos`` / ``make_gpu_reactions`` — gpuThermo/makeGpuThermo.H:16-66
+    and gpuReaction/makeGpuReactions.H:18-142 (x R scaling, reaction ΔThermo,
+    integer-exponent detection) on a RawMechanism instead of OpenFOAM dictionaries;
+  * ``GpuKernelEvaluator`` — gpuKernelEvaluator/gpuKernelEvaluator.H:18-85:
+    ``computeYNew`` and ``computeRR`` with the same arguments, results and error
+    behaviour (an unknown solver name raises, as make_gpuODESolver throws).
+
+Device memory and streams come from PyTorch; the computation is the CUDA path
+of libgpufoam_b200.so. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from .mechanism import RATE_ARRHENIUS, RawMechanism
+
+_SOLVERS = {"Rosenbrock12": 12, "Rosenbrock23": 23, "Rosenbrock34": 34}
+_DBL_EPS = np.finfo(np.float64).eps
+
+
+@dataclasses.dataclass
+class OdeInputs:
+    """gpuODESolverInputs (gpuOde/gpuODESolverInputs.H:9-23)."""
+    name: str = "Rosenbrock34"
+    absTol: float = _DBL_EPS
+    relTol: float = 1e-4
+    maxSteps: int = 10000
+    safeScale: float = 0.9
+    alphaInc: float = 0.2
+    alphaDec: float = 0.25
+    minScale: float = 0.2
+    maxScale: float = 10.0
+
+    def to_c(self) -> N.GfOdeInputs:
+        if self.name not in _SOLVERS:
+            # make_gpuODESolver throws std::logic_error (makeGpuOdeSolver.H:28)
+            raise ValueError("Invalid ODE Solver type")
+        return N.GfOdeInputs(_SOLVERS[self.name], self.absTol, self.relTol, int(self.maxSteps), self.safeScale,
+                             self.alphaInc, self.alphaDec, self.minScale, self.maxScale)
+
+
+def read_gpuODESolverInputs(d: dict) -> OdeInputs:
+    """odeCoeffs dictionary -> OdeInputs, with the reference's defaults."""
+    return OdeInputs(name=d["solver"], absTol=d.get("absTol", _DBL_EPS), relTol=d.get("relTol", 1e-4),
+                     maxSteps=int(d.get("maxSteps", 10000)), safeScale=d.get("safeScale", 0.9),
+                     alphaInc=d.get("alphaIncrease", 0.2), alphaDec=d.get("alphaDecrease", 0.25),
+                     minScale=d.get("minScale", 0.2), maxScale=d.get("maxScale", 10.0))
+
+
+def is_integer(x: float) -> bool:
+    """isInteger (gpuReaction/gpuSpecieExponent.H:7-19): truncate, integer unless positive remainder."""
+    X = int(x)
+    return not (x - X > 0)
+
+
+def make_gpu_thermos(mech: RawMechanism):
+    lib = N.load()
+    arr = (N.GfThermo * mech.n_species)()
+    for i in range(mech.n_species):
+        hi = (C.c_double * 7)(*mech.high_raw[i])
+        lo = (C.c_double * 7)(*mech.low_raw[i])
+        N.check(lib.gf_thermo_from_nasa(1.0, float(mech.W[i]), float(mech.Tlow[i]), float(mech.Thigh[i]),
+                                        float(mech.Tcommon[i]), hi, lo, C.byref(arr[i])), "gf_thermo_from_nasa")
+    return arr
+
+
+def _coeffs(side):
+    out = (N.GfSpecieCoeff * N.GF_MAX_REACTION_WIDTH)()
+    if len(side) > N.GF_MAX_REACTION_WIDTH:
+        raise ValueError("Too long reaction")
+    for k, (idx, st, ex) in enumerate(side):
+        integer = is_integer(ex)
+        out[k] = N.GfSpecieCoeff(int(idx), int(integer), float(st), float(int(ex)) if integer else float(ex))
+    return out
+
+
+def make_gpu_reactions(mech: RawMechanism, thermos):
+    lib = N.load()
+    arr = (N.GfReaction * max(mech.n_reactions, 1))()
+    keep = []
+    for r, rx in enumerate(mech.reactions):
+        g = arr[r]
+        g.n_lhs, g.n_rhs = len(rx.lhs), len(rx.rhs)
+        g.lhs = _coeffs(rx.lhs)
+        g.rhs = _coeffs(rx.rhs)
+        N.check(lib.gf_reaction_thermo(thermos, mech.n_species, g.n_lhs, g.lhs, g.n_rhs, g.rhs, C.byref(g.thermo)),
+                "gf_reaction_thermo")
+        g.rate_type = rx.rate_type
+        g.irreversible = int(rx.irreversible)
+        g.A, g.beta, g.Ta = rx.A, rx.beta, rx.Ta
+        g.Ainf, g.betainf, g.Tainf = rx.Ainf, rx.betainf, rx.Tainf
+        g.troe_alpha, g.troe_Tsss, g.troe_Ts, g.troe_Tss = rx.troe
+        if rx.rate_type != RATE_ARRHENIUS:
+            e = np.ascontiguousarray(rx.efficiencies, dtype=np.float64)
+            keep.append(e)
+            g.efficiencies = e.ctypes.data_as(C.POINTER(C.c_double))
+        g.Tlow, g.Thigh = mech.rxn_Tlow, mech.rxn_Thigh
+    return arr, keep
+
+
+def thermo_table(arr, n) -> np.ndarray:
+    """[n][19] = Y, W, Tlow, Thigh, Tcommon, high[7], low[7] (the oracle's table layout)."""
+    out = np.zeros((n, 19))
+    for i in range(n):
+        t = arr[i]
+        if isinstance(t, N.GfReaction):
+            t = t.thermo
+        out[i, :5] = (t.Y, t.W, t.Tlow, t.Thigh, t.Tcommon)
+        out[i, 5:12] = list(t.high)
+        out[i, 12:19] = list(t.low)
+    return out
+
+
+class Mechanism:
+    """Device-resident mechanism tables (gf_mech)."""
+
+    def __init__(self, raw: RawMechanism):
+        import torch  # noqa: F401  (initialises the CUDA context torch shares)
+        self.raw = raw
+        self.lib = N.load()
+        self.thermos = make_gpu_thermos(raw)
+        self.reactions, self._keep = make_gpu_reactions(raw, self.thermos)
+        desc = N.GfMechDesc(raw.n_species, raw.n_reactions, self.thermos, self.reactions)
+        h = C.c_void_p()
+        N.check(self.lib.gf_mech_create(C.byref(desc), C.byref(h)), "gf_mech_create")
+        self.handle = h
+        self.n_species = raw.n_species
+        self.n_reactions = raw.n_reactions
+        self.n_eqns = raw.n_species + 2
+
+    def tables(self):
+        return thermo_table(self.thermos, self.n_species), thermo_table(self.reactions, self.n_reactions)
+
+    def device_bytes(self) -> int:
+        b = C.c_longlong()
+        N.check(self.lib.gf_mech_info(self.handle, None, None, C.byref(b)), "gf_mech_info")
+        return b.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.gf_mech_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dev(x, dtype=None):
+    import torch
+    t = torch.as_tensor(x)
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.to("cuda").contiguous()
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Solver:
+    """gf_solver: one or more mechanisms + ODE inputs + Treact + launch form."""
+
+    def __init__(self, mechs: Sequence[Mechanism], ode: OdeInputs, Treact: float = 0.0):
+        self.lib = N.load()
+        self.mechs = list(mechs)
+        arr = (C.c_void_p * len(self.mechs))(*[m.handle.value for m in self.mechs])
+        h = C.c_void_p()
+        N.check(self.lib.gf_solver_create(arr, len(self.mechs), C.byref(ode.to_c()), float(Treact), C.byref(h)),
+                "gf_solver_create")
+        self.handle = h
+        self.ode = ode
+        self.Treact = Treact
+        self.max_neq = max(m.n_eqns for m in self.mechs)
+
+    def set_launch(self, kind=1, threads_per_cell=32, scratch_in_shared=1, cells_per_block=0, blocks_per_sm=0,
+                   register_budget=0):
+        cfg = N.GfLaunchConfig(kind, threads_per_cell, scratch_in_shared, cells_per_block, blocks_per_sm,
+                               register_budget)
+        N.check(self.lib.gf_solver_set_launch(self.handle, C.byref(cfg)), "gf_solver_set_launch")
+
+    def get_launch(self) -> dict:
+        cfg = N.GfLaunchConfig()
+        N.check(self.lib.gf_solver_get_launch(self.handle, C.byref(cfg)), "gf_solver_get_launch")
+        return cfg.as_dict()
+
+    def solve(self, Y0, deltaT: float, deltaTChem, deltaTChemMax: float = np.inf, rho=None, deltaT_cell=None,
+              mech_id=None, Ynew=None, RR=None, want_status=True, want_counters=True, want_stats=True,
+              stream=None):
+        """Device-tensor solve (gf_solve). Y0 [n][ld] float64 cuda; deltaTChem [n] is updated in place.
+        Returns dict(Ynew, RR, deltaTChem, status, counters, stats)."""
+        import torch
+        n = int(Y0.shape[0])
+        ld = int(Y0.shape[1])
+        if Ynew is None:
+            Ynew = torch.empty_like(Y0)
+        if rho is not None and RR is None:
+            RR = torch.empty((n, ld), dtype=torch.float64, device=Y0.device)
+        status = torch.empty(n, dtype=torch.int32, device=Y0.device) if want_status else None
+        counters = torch.empty((n, 2), dtype=torch.int32, device=Y0.device) if want_counters else None
+        st = N.GfStats()
+        N.check(self.lib.gf_solve(self.handle, n, float(deltaT), _ptr(deltaT_cell), float(deltaTChemMax),
+                                  _ptr(mech_id), _ptr(rho), _ptr(Y0), ld, _ptr(Ynew), _ptr(deltaTChem), _ptr(RR),
+                                  ld if RR is not None else 0, _ptr(status), _ptr(counters),
+                                  C.byref(st) if want_stats else None, _stream_ptr(stream)), "gf_solve")
+        return dict(Ynew=Ynew, RR=RR, deltaTChem=deltaTChem, status=status, counters=counters,
+                    stats=dict(accepted=st.accepted_steps, attempts=st.attempts, failed=st.failed_cells,
+                               min_delta_t=st.min_delta_t) if want_stats else None)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.gf_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuKernelEvaluator:
+    """Mirror of FoamGpu::GpuKernelEvaluator (gpuKernelEvaluator.H:18-85).
+
+    GpuKernelEvaluator(nCells, nEqns, nSpecie, mechanism, odeInputs, Treact=0)
+    where ``mechanism`` replaces the reference's (thermos, reactions) vectors.
+    Inputs and outputs are host arrays, as in the reference."""
+
+    def __init__(self, nCells: int, nEqns: int, nSpecie: int, mechanism, odeInputs: OdeInputs,
+                 Treact: float = 0.0):
+        if isinstance(mechanism, RawMechanism):
+            mechanism = Mechanism(mechanism)
+        if nEqns != nSpecie + 2 or mechanism.n_species != nSpecie:
+            raise ValueError("nEqns must be nSpecie + 2 and match the mechanism")
+        self.nCells, self.nEqns, self.nSpecie = nCells, nEqns, nSpecie
+        self.mechanism = mechanism
+        self.solver = Solver([mechanism], odeInputs, Treact)
+        self.lib = self.solver.lib
+
+    def computeYNew(self, deltaT: float, deltaTChemMax: float, deltaTChem, Y):
+        """-> (Ynew [nCells*nEqns], deltaTChemNew [nCells]) (gpuKernelEvaluator.cu:35-63)."""
+        dtc = np.ascontiguousarray(deltaTChem, dtype=np.float64)
+        Yh = np.ascontiguousarray(Y, dtype=np.float64).reshape(-1)
+        n = dtc.shape[0]
+        Ynew = np.empty(n * self.nEqns)
+        dtn = np.empty(n)
+        N.check(self.lib.gf_compute_ynew(self.solver.handle, n, float(deltaT), float(deltaTChemMax),
+                                         dtc.ctypes.data, Yh.ctypes.data, Ynew.ctypes.data, dtn.ctypes.data),
+                "gf_compute_ynew")
+        return Ynew, dtn
+
+    def computeRR(self, deltaT: float, deltaTChemMax: float, rho, deltaTChem, Y):
+        """-> (RR [nCells*nSpecie], deltaTChemNew [nCells] clamped, minDeltaT)
+        (gpuKernelEvaluator.cu:65-97)."""
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        dtc = np.ascontiguousarray(deltaTChem, dtype=np.float64)
+        Yh = np.ascontiguousarray(Y, dtype=np.float64).reshape(-1)
+        n = rho.shape[0]
+        RR = np.empty(n * self.nSpecie)
+        dtn = np.empty(n)
+        mn = C.c_double()
+        N.check(self.lib.gf_compute_rr(self.solver.handle, n, float(deltaT), float(deltaTChemMax), rho.ctypes.data,
+                                       dtc.ctypes.data, Yh.ctypes.data, RR.ctypes.data, dtn.ctypes.data,
+                                       C.byref(mn)), "gf_compute_rr")
+        return RR, dtn, mn.value
+
+
+# ---- parity entry points ----------------------------------------------------
+
+def rates(mech: Mechanism, y):
+    """derivatives(y) for states y [n][nEqns] (host or device) -> cuda tensor."""
+    import torch
+    yd = _dev(y, torch.float64)
+    out = torch.empty_like(yd)
+    N.check(mech.lib.gf_rates(mech.handle, yd.shape[0], _ptr(yd), _ptr(out), _stream_ptr()), "gf_rates")
+    return out
+
+
+def jacobian(mech: Mechanism, y):
+    import torch
+    yd = _dev(y, torch.float64)
+    n = yd.shape[1]
+    dfdx = torch.empty_like(yd)
+    J = torch.empty((yd.shape[0], n, n), dtype=torch.float64, device="cuda")
+    N.check(mech.lib.gf_jacobian(mech.handle, yd.shape[0], _ptr(yd), _ptr(dfdx), _ptr(J), _stream_ptr()),
+            "gf_jacobian")
+    return dfdx, J
+
+
+def lu_decompose(A):
+    import torch
+    lib = N.load()
+    Ad = _dev(A, torch.float64).clone()
+    k, m, _ = Ad.shape
+    piv = torch.empty((k, m), dtype=torch.int32, device="cuda")
+    N.check(lib.gf_lu_decompose(k, m, _ptr(Ad), _ptr(piv), _stream_ptr()), "gf_lu_decompose")
+    return Ad, piv
+
+
+def lu_backsubstitute(LU, piv, b):
+    import torch
+    lib = N.load()
+    bd = _dev(b, torch.float64).clone()
+    k, m = bd.shape
+    N.check(lib.gf_lu_backsubstitute(k, m, _ptr(_dev(LU, torch.float64)), _ptr(_dev(piv, torch.int32)), _ptr(bd),
+                                     _stream_ptr()), "gf_lu_backsubstitute")
+    return bd

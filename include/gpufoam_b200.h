@@ -142,9 +142,10 @@ typedef struct gf_launch_config {
     int kind;
     int threads_per_cell;    /* 1, 2, 4, 8, 16 or 32 (persistent only)          */
     int scratch_in_shared;   /* 1: per-cell workspace in shared memory           */
-    int cells_per_block;     /* groups per CTA (persistent only)                 */
+    int cells_per_block;     /* groups per CTA (persistent only; CTAs have at most 128 threads) */
     int blocks_per_sm;       /* 0 = as many as fit                               */
-    int lu_block;            /* reserved, 0                                      */
+    int register_budget;     /* persistent only: 0 = up to 255 registers per thread,
+                                1 = at most 128 (more resident cell groups)      */
 } gf_launch_config;
 
 typedef struct gf_stats {
@@ -235,6 +236,13 @@ int gf_lu_decompose(int n_mats, int m, double* A, int* pivots, void* stream);
 /* In-place solve of b [n_mats][m] with the factors from gf_lu_decompose. */
 int gf_lu_backsubstitute(int n_mats, int m, const double* LU, const int* pivots,
                          double* b, void* stream);
+
+/* ---- measurement (no reference counterpart) -------------------------------- */
+
+/* FP64 FMA throughput of the current device, measured with independent DFMA
+ * chains for about `ms` milliseconds: the roofline denominator of the kernels
+ * above, which run on the FP64 CUDA-core pipe. */
+int gf_measure_fp64_peak(double ms, double* tflops);
 
 /* ---- misc --------------------------------------------------------------- */
 const char* gf_strerror(int status);

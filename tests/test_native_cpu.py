@@ -1,0 +1,93 @@
+"""CPU checks of the C-ABI library: it loads, exports every declared symbol, and
+its host-side loader arithmetic (makeGpuThermo x R scaling, set_reaction_thermo
+ΔThermo, integer-exponent detection) reproduces the reference's processed
+tables bit for bit. No compute call needs a GPU here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from gpufoam_b200 import _native as N
+from gpufoam_b200 import build as B
+from gpufoam_b200 import evaluator as E
+from gpufoam_b200 import mechanism as M
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+@pytest.fixture(scope="module")
+def lib():
+    B.build()
+    return N.load()
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "gpufoam_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(gf_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_exports_every_declared_symbol(lib):
+    syms = header_symbols()
+    assert len(syms) >= 19
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) == set(N.EXPORTS)
+    assert lib.gf_abi_version() == 1
+
+
+def test_strerror(lib):
+    assert lib.gf_strerror(0) == b"ok"
+    assert lib.gf_strerror(2) == b"Invalid ODE Solver type"
+
+
+@pytest.mark.parametrize("name", ["h2size", "coverage", "grisize"])
+def test_loader_arithmetic_matches_reference_tables(lib, name):
+    from tests.test_oracle import fixture_mech
+    g = dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
+    mech = fixture_mech(g)
+    th = E.make_gpu_thermos(mech)
+    rx, _keep = E.make_gpu_reactions(mech, th)
+    assert np.array_equal(E.thermo_table(th, mech.n_species), g["species_tables"])
+    assert np.array_equal(E.thermo_table(rx, mech.n_reactions), g["reaction_tables"])
+    ie = g["int_exponents"]
+    for r in range(mech.n_reactions):
+        for k in range(rx[r].n_lhs):
+            assert rx[r].lhs[k].integer_exponent == ie[r, k]
+        for k in range(rx[r].n_rhs):
+            assert rx[r].rhs[k].integer_exponent == ie[r, 10 + k]
+
+
+def test_mass_imbalance_rejected(lib):
+    mech = M.h2_size(0)
+    th = E.make_gpu_thermos(mech)
+    lhs = (N.GfSpecieCoeff * 10)()
+    rhs = (N.GfSpecieCoeff * 10)()
+    lhs[0] = N.GfSpecieCoeff(0, 1, 1.0, 1.0)   # H
+    rhs[0] = N.GfSpecieCoeff(4, 1, 1.0, 1.0)   # O2: not balanced
+    out = N.GfThermo()
+    assert lib.gf_reaction_thermo(th, mech.n_species, 1, lhs, 1, rhs, C.byref(out)) == 4
+
+
+def test_unknown_solver_rejected(lib):
+    assert lib.gf_solver_create(None, 1, None, 0.0, None) == 1
+    fake = (C.c_void_p * 1)(C.c_void_p(0x1000).value)
+    ode = N.GfOdeInputs(99, 1e-8, 1e-4, 10000, 0.9, 0.2, 0.25, 0.2, 10.0)
+    h = C.c_void_p()
+    assert lib.gf_solver_create(fake, 1, C.byref(ode), 0.0, C.byref(h)) == 2
+    with pytest.raises(ValueError, match="Invalid ODE Solver type"):
+        E.OdeInputs(name="seulex").to_c()
+
+
+def test_ode_input_defaults():
+    o = E.read_gpuODESolverInputs({"solver": "Rosenbrock23"})
+    assert (o.absTol, o.relTol, o.maxSteps, o.safeScale, o.alphaInc, o.alphaDec, o.minScale, o.maxScale) == (
+        np.finfo(float).eps, 1e-4, 10000, 0.9, 0.2, 0.25, 0.2, 10.0)
+
+
+def test_is_integer_rule():
+    # isInteger truncates toward zero and only rejects a positive remainder
+    assert E.is_integer(2.0) and E.is_integer(-0.5) and not E.is_integer(1.5)
