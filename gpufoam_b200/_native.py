@@ -28,7 +28,7 @@ EXPORTS = [
     "gf_thermo_from_nasa", "gf_reaction_thermo", "gf_mech_create", "gf_mech_destroy", "gf_mech_info",
     "gf_solver_create", "gf_solver_destroy", "gf_solver_set_launch", "gf_solver_get_launch", "gf_solve",
     "gf_compute_rr", "gf_compute_ynew", "gf_rates", "gf_jacobian", "gf_lu_decompose", "gf_lu_backsubstitute",
-    "gf_strerror", "gf_abi_version", "gf_last_cuda_error", "gf_measure_fp64_peak",
+    "gf_strerror", "gf_abi_version", "gf_last_cuda_error", "gf_measure_fp64_peak", "gf_solve_noalloc",
 ]
 
 
@@ -124,6 +124,8 @@ def load() -> C.CDLL:
     lib.gf_lu_decompose.argtypes = [ip, ip, vp, vp, vp]
     lib.gf_lu_backsubstitute.argtypes = [ip, ip, vp, vp, vp, vp]
     lib.gf_measure_fp64_peak.argtypes = [dp, P(dp)]
+    lib.gf_solve_noalloc.argtypes = [vp, P(GfOdeInputs), dp, ip, dp, vp, dp, vp, vp, ip, vp, vp, vp, ip, vp, vp,
+                                     P(GfStats), vp]
     lib.gf_strerror.argtypes = [ip]
     lib.gf_strerror.restype = C.c_char_p
     lib.gf_abi_version.restype = ip

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libgpufoam_b200.so")
-SOURCES = ["gf_host.cpp", "gf_kernels.cu", "gf_peak.cu"]
+SOURCES = ["gf_host.cpp", "gf_kernels.cu", "gf_peak.cu", "gf_noalloc.cu"]
 HEADERS = ["gf_internal.h", "gf_device.cuh", os.path.join("..", "..", "include", "gpufoam_b200.h")]
 
 NVCC_FLAGS = [

@@ -132,6 +132,10 @@ struct gf_solver {
     int staged_cells = 0;
 };
 
+namespace gf {
+const DevMech* mech_device_tables(const gf_mech* m) { return &m->dev; }
+}  // namespace gf
+
 namespace {
 
 int ensure_ws(gf_solver* s, size_t bytes) {

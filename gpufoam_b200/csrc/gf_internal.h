@@ -142,6 +142,9 @@ int launch_lu(int n_mats, int m, double* A, int* piv, double* vv, void* stream);
 int launch_lusolve(int n_mats, int m, const double* LU, const int* piv, double* b, void* stream);
 int launch_epilogue_reset(unsigned long long* queue, void* stream);
 
+// Device tables of a mechanism object (gf_host.cpp).
+const DevMech* mech_device_tables(const gf_mech* m);
+
 // Resident-slot count for a persistent configuration (groups that run at once).
 int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* blocks_out, int* threads_out);
 int device_sm_count();

@@ -282,6 +282,28 @@ class GpuKernelEvaluator:
         return RR, dtn, mn.value
 
 
+def solve_noalloc(mech: Mechanism, ode: OdeInputs, Y0, deltaT: float, deltaTChem, Ynew, Treact: float = 0.0,
+                  deltaTChemMax: float = np.inf, rho=None, RR=None, status=None, counters=None, stats=True,
+                  stream=None):
+    """gf_solve_noalloc: the solve for callers that cannot allocate device
+    memory. Every array is the caller's (cuda tensors); deltaTChem is updated
+    in place and Ynew/RR/status/counters are written. The library's static
+    device scratch is shared by all calls, so calls must not overlap on a GPU.
+    Returns the statistics dict when stats=True (this synchronises the stream)."""
+    lib = N.load()
+    n = int(Y0.shape[0])
+    st = N.GfStats()
+    N.check(lib.gf_solve_noalloc(mech.handle, C.byref(ode.to_c()), float(Treact), n, float(deltaT), None,
+                                 float(deltaTChemMax), _ptr(rho), _ptr(Y0), int(Y0.shape[1]), _ptr(Ynew),
+                                 _ptr(deltaTChem), _ptr(RR), int(RR.shape[1]) if RR is not None else 0,
+                                 _ptr(status), _ptr(counters), C.byref(st) if stats else None, _stream_ptr(stream)),
+            "gf_solve_noalloc")
+    if stats:
+        return dict(accepted=st.accepted_steps, attempts=st.attempts, failed=st.failed_cells,
+                    min_delta_t=st.min_delta_t)
+    return None
+
+
 # ---- parity entry points ----------------------------------------------------
 
 def rates(mech: Mechanism, y):

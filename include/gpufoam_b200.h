@@ -222,6 +222,26 @@ int gf_compute_ynew(gf_solver* solver, int n_cells, double deltaT, double deltaT
                     const double* deltaTChem, const double* Y, double* Ynew,
                     double* deltaTChemNew);
 
+/* Size of the static device scratch of gf_solve_noalloc (32 MiB per GPU). */
+#define GF_NOALLOC_SCRATCH_BYTES (32ll * 1024 * 1024)
+
+/* gf_solve without any device allocation — no counterpart in the reference.
+ * For callers that cannot call cudaMalloc: code that runs while a CUDA graph is
+ * captured, host codes whose device memory belongs to another allocator,
+ * loops that forbid allocation after start-up. The mechanism (gf_mech_create)
+ * is set-up-time input; inputs and outputs are the caller's device arrays, as
+ * in gf_solve. The per-cell workspaces and work-queue counters live in a static
+ * device array of GF_NOALLOC_SCRATCH_BYTES that every GPU loading the library
+ * holds until exit; the number of cells integrated at once is capped so their
+ * workspaces fit (GF_ERR_UNSUPPORTED if not even one cell's does). The first
+ * call on each device resolves the array's address (cudaGetSymbolAddress) and
+ * should come before any stream capture. All calls share the array: calls
+ * whose kernels overlap on one GPU race and must not be issued. */
+int gf_solve_noalloc(const gf_mech* mech, const gf_ode_inputs* inputs, double Treact, int n_cells, double deltaT,
+                     const double* deltaT_cell, double deltaTChemMax, const double* rho, const double* Y0, int ld_y,
+                     double* Ynew, double* deltaTChem, double* RR, int ld_rr, int* status, int* counters,
+                     gf_stats* stats, void* stream);
+
 /* ---- parity entry points (one thread group per state, device pointers) --- */
 
 /* dydx [n_states][nEqns] = derivatives(y [n_states][nEqns]). */
