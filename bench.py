@@ -61,11 +61,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="gri-100k", choices=list(WORKLOADS))
     ap.add_argument("--solver", type=int, default=34, choices=[12, 23, 34])
-    ap.add_argument("--launch", default="fixed", choices=["fixed", "auto", "sweep"],
+    ap.add_argument("--launch", default="auto", choices=["fixed", "auto", "sweep"],
                     help="fixed: --threads-per-cell/--shared; auto: autotuner on a sample; "
                          "sweep: print every launch form's time to stderr, then use the best")
-    ap.add_argument("--threads-per-cell", type=int, default=32)
+    ap.add_argument("--threads-per-cell", type=int, default=64)
     ap.add_argument("--shared", type=int, default=1)
+    ap.add_argument("--register-budget", type=int, default=0, choices=[0, 1],
+                    help="persistent kernel: 0 = up to 255 registers per thread, 1 = at most 128")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -240,7 +242,8 @@ def main():
     N.check(lib.gf_measure_fp64_peak(200.0, ctypes.byref(peak)), "gf_measure_fp64_peak")
 
     solver = E.Solver([mech], ode)
-    solver.set_launch(kind=1, threads_per_cell=args.threads_per_cell, scratch_in_shared=args.shared)
+    solver.set_launch(kind=1, threads_per_cell=args.threads_per_cell, scratch_in_shared=args.shared,
+                      register_budget=args.register_budget)
     tuned = None
     if args.launch != "fixed":
         from gpufoam_b200 import autotune
@@ -282,7 +285,7 @@ def main():
     e2e = None
     if not args.no_e2e:
         ev = E.GpuKernelEvaluator(n, raw.n_eqns, raw.n_species, mech, ode)
-        ev.solver.set_launch(kind=1, threads_per_cell=args.threads_per_cell, scratch_in_shared=args.shared)
+        ev.solver.set_launch(**solver.get_launch())
         hY = torch.empty((n, raw.n_eqns), dtype=torch.float64, pin_memory=True)
         hY.copy_(torch.as_tensor(cells))
         hrho = torch.empty(n, dtype=torch.float64, pin_memory=True)

@@ -35,7 +35,19 @@ constexpr int kMaxRejects = 100000;  // rejected attempts within one substep
 // Built only with -DGF_PHASE_TIMERS (a profiling variant of the library):
 // lane 0 of each group accumulates clock64() cycles per phase of the solve.
 #ifdef GF_PHASE_TIMERS
-__device__ unsigned long long g_phase_cycles[16];
+// one accumulator per translation unit (each has its own device module)
+static __device__ unsigned long long g_phase_cycles[16];
+// adds this translation unit's accumulators to out[16], optionally clearing them
+static inline int phase_cycles_local(unsigned long long* out, int reset) {
+    unsigned long long v[16];
+    cudaMemcpyFromSymbol(v, g_phase_cycles, sizeof(v));
+    for (int i = 0; i < 16; ++i) out[i] += v[i];
+    if (reset) {
+        unsigned long long z[16] = {};
+        cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
+    }
+    return (int)cudaGetLastError();
+}
 #define GF_PH_BEGIN(g) \
     (g).sync();        \
     const long long _gf_ph0 = clock64();
@@ -51,39 +63,84 @@ enum { PH_MIX = 0, PH_NMPOW, PH_OMEGA, PH_GATHER_RHS, PH_JPARAMS, PH_JROWS, PH_T
 
 // ---------------------------------------------------------------- groups
 
+// Cross-warp reduction buffer of a multi-warp group (one group per CTA).
+__device__ __forceinline__ double* grp_red_buf() {
+    __shared__ double buf[8];
+    return buf;
+}
+
+// G <= 32: G aligned lanes of one warp, several groups per warp/CTA.
+// G = 64, 128, 256: the whole CTA (one cell per CTA); barriers are
+// __syncthreads and reductions go through a small shared buffer, in a fixed
+// warp order (deterministic).
 template <int G>
 struct Grp {
+    static constexpr int W = G > 32 ? G / 32 : 1;  // warps in the group
     int lane;
     unsigned mask;
     __device__ __forceinline__ Grp() {
         const int wl = threadIdx.x & 31;
-        lane = wl & (G - 1);
-        mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (wl & ~(G - 1)));
+        if constexpr (G >= 32) {
+            lane = G > 32 ? (int)threadIdx.x : wl;
+            mask = 0xffffffffu;
+        } else {
+            lane = wl & (G - 1);
+            mask = ((1u << G) - 1u) << (wl & ~(G - 1));
+        }
     }
     __device__ __forceinline__ void sync() const {
-        if (G > 1) __syncwarp(mask);
-    }
-    __device__ __forceinline__ double bcast(double v, int src) const {
-        if (G == 1) return v;
-        return __shfl_sync(mask, v, src, G);
+        if (G > 32)
+            __syncthreads();
+        else if (G > 1)
+            __syncwarp(mask);
     }
     __device__ __forceinline__ long long bcast_ll(long long v, int src) const {
         if (G == 1) return v;
+        if (G > 32) {
+            long long* b = reinterpret_cast<long long*>(grp_red_buf());
+            __syncthreads();
+            if (lane == src) b[0] = v;
+            __syncthreads();
+            v = b[0];
+            __syncthreads();
+            return v;
+        }
         return __shfl_sync(mask, v, src, G);
     }
     __device__ __forceinline__ double sum(double v) const {
+        constexpr int L = G > 32 ? 32 : G;
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
+        for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, L);
+        if (G > 32) {
+            double* b = grp_red_buf();
+            if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+            __syncthreads();
+            v = b[0];
+#pragma unroll
+            for (int k = 1; k < W; ++k) v += b[k];
+            __syncthreads();
+        }
         return v;
     }
     // max with fmax semantics: a NaN operand is ignored (normaliseError.H:22)
     __device__ __forceinline__ double fmax_(double v) const {
+        constexpr int L = G > 32 ? 32 : G;
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o, G));
+        for (int o = L / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o, L));
+        if (G > 32) {
+            double* b = grp_red_buf();
+            if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+            __syncthreads();
+            v = b[0];
+#pragma unroll
+            for (int k = 1; k < W; ++k) v = fmax(v, b[k]);
+            __syncthreads();
+        }
         return v;
     }
     __device__ __forceinline__ int any(int p) const {
         if (G == 1) return p;
+        if (G > 32) return __syncthreads_or(p) != 0;
         return (__ballot_sync(mask, p) & mask) != 0;
     }
 };
@@ -253,21 +310,62 @@ __device__ __forceinline__ double arr_dlnkdT(const DevMech& M, int q, int f, con
     return (beta + Ta * tc.invT) * tc.invT;  // (beta + Ta/T)/T
 }
 
-// third-body concentration M = sum eff_i c_i (gpuThirdBodyEfficiencies.H:28-35)
-// (species-major table: the lanes of a warp, each on its own reaction, read
-// consecutive addresses; two partial sums for latency)
-template <class W>
-__device__ __forceinline__ double third_body_M(const DevMech& M, int q, const W& w, int c_off) {
-    const double* e = M.eff_t + ldg(M.tb_row + q);
-    const int st = M.n_tb;
-    double s0 = 0, s1 = 0;
-    int i = 0;
-    for (; i + 1 < M.nS; i += 2) {
-        s0 += ldg(e + (size_t)i * st) * w[c_off + i];
-        s1 += ldg(e + (size_t)(i + 1) * st) * w[c_off + i + 1];
+// Third-body concentrations M_t = sum_i eff_ti c_i of every third-body and
+// fall-off reaction (gpuThirdBodyEfficiencies.H:28-35), written to Mtb[t]:
+// lanes over species (coalesced rows of eff), warps over reactions, rows in
+// batches of 8 so that their loads are in flight together; each sum is
+// lane-strided and combined by a fixed shuffle tree (deterministic; the
+// reference sums sequentially, an ulp-level reordering).
+template <int G, class W>
+__device__ __forceinline__ void third_body_all(const Grp<G>& g, const DevMech& M, const W& w, int c_off, int m_off) {
+    constexpr int LW = G > 32 ? 32 : G;
+    constexpr int NW = G > 32 ? G / 32 : 1;
+    constexpr int RB = 8;
+    constexpr int SPL = 3;  // species per lane held at once: nS <= SPL * LW, else looped
+    const int rg = G > 32 ? (g.lane >> 5) : 0;
+    const int rl = G > 32 ? (g.lane & 31) : g.lane;
+    const unsigned mask = G > 32 ? 0xffffffffu : g.mask;
+    const int nS = M.nS;
+    for (int t0 = rg * RB; t0 < M.n_tb; t0 += NW * RB) {
+        double sum[RB];
+        if (nS <= SPL * LW) {
+            double cv[SPL];
+#pragma unroll
+            for (int k = 0; k < SPL; ++k) {
+                const int i = rl + k * LW;
+                cv[k] = i < nS ? w[c_off + i] : 0.0;
+            }
+            double e[RB][SPL];
+#pragma unroll
+            for (int b = 0; b < RB; ++b)
+#pragma unroll
+                for (int k = 0; k < SPL; ++k) {
+                    const int i = rl + k * LW;
+                    e[b][k] = (t0 + b < M.n_tb && i < nS) ? ldg(M.eff + (size_t)(t0 + b) * nS + i) : 0.0;
+                }
+#pragma unroll
+            for (int b = 0; b < RB; ++b) {
+                double acc = 0.0;
+#pragma unroll
+                for (int k = 0; k < SPL; ++k) acc += e[b][k] * cv[k];
+                sum[b] = acc;
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < RB; ++b) {
+                double acc = 0.0;
+                if (t0 + b < M.n_tb)
+                    for (int i = rl; i < nS; i += LW) acc += ldg(M.eff + (size_t)(t0 + b) * nS + i) * w[c_off + i];
+                sum[b] = acc;
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < RB; ++b) {
+#pragma unroll
+            for (int o = LW / 2; o > 0; o >>= 1) sum[b] += __shfl_xor_sync(mask, sum[b], o, LW);
+            if (rl == 0 && t0 + b < M.n_tb) w[m_off + t0 + b] = sum[b];
+        }
     }
-    if (i < M.nS) s0 += ldg(e + (size_t)i * st) * w[c_off + i];
-    return s0 + s1;
 }
 
 // Troe F (gpuTroeFallOffFunction.H:27-47); troe[] holds alpha, 1/T***, 1/T*, T**
@@ -292,8 +390,9 @@ __device__ __forceinline__ double troe_F(const DevMech& M, int q, const TCache& 
 // want_dT also dkf/dT and, for third-body rates, the pure Arrhenius part Ak
 // ("everything", gpuArrheniusReactionRate.H:97-107,
 // gpuThirdBodyArrheniusReactionRate.H:105-121, gpuFallOffReactionRate.H:127-158).
-template <class W>
-__device__ __forceinline__ double rate_k(const DevMech& M, int q, int type, const TCache& tc, const W& w, int c_off,
+// Mc: the reaction's third-body concentration (third_body_all), unused for
+// plain Arrhenius rates.
+__device__ __forceinline__ double rate_k(const DevMech& M, int q, int type, const TCache& tc, double Mc,
                                          bool want_dT, double* dT_out, double* Ak_out) {
     if (type == GF_RATE_ARRHENIUS) {
         const double Ak = ldg(M.sA0 + q) * exp(arr_ln(M, q, 0, tc));
@@ -302,7 +401,6 @@ __device__ __forceinline__ double rate_k(const DevMech& M, int q, int type, cons
     }
     if (type == GF_RATE_THIRD_BODY_ARRHENIUS) {
         const double Ak = ldg(M.sA0 + q) * exp(arr_ln(M, q, 0, tc));
-        const double Mc = third_body_M(M, q, w, c_off);
         if (want_dT) *dT_out = Mc * (Ak * arr_dlnkdT(M, q, 0, tc));
         *Ak_out = Ak;
         return Mc * Ak;
@@ -311,7 +409,6 @@ __device__ __forceinline__ double rate_k(const DevMech& M, int q, int type, cons
     const double l0 = arr_ln(M, q, 0, tc), l1 = arr_ln(M, q, 1, tc);
     const double s0 = ldg(M.sA0 + q), s1 = ldg(M.sA1 + q);
     const double kInf = s1 * exp(l1);
-    const double Mc = third_body_M(M, q, w, c_off);
     const double Pr = (s0 * s1) * exp(l0 - l1) * Mc;
     const double F = type == GF_RATE_TROE_FALLOFF ? troe_F(M, q, tc, Pr) : 1.0;
     const double temp = (Pr / (1.0 + Pr)) * F;
@@ -321,7 +418,7 @@ __device__ __forceinline__ double rate_k(const DevMech& M, int q, int type, cons
 
 // ------------------------------------------------------------- layout
 
-__host__ __device__ inline WsLayout make_layout(int nS, int nR, int n_slots) {
+__host__ __device__ inline WsLayout make_layout(int nS, int nR, int n_slots, int n_tb) {
     WsLayout L;
     const int m = nS + 1;
     L.ld = m | 1;
@@ -345,8 +442,8 @@ __host__ __device__ inline WsLayout make_layout(int nS, int nR, int n_slots) {
     L.Ha = o; o += nS;
     L.rhoMbyW = o; o += nS;
     L.vj = o; o += nS;
-    L.kcache = o; o += 3 * (nR > 0 ? nR : 1);
     L.stage = o; o += (n_slots > 0 ? n_slots : 1);
+    L.Mtb = o; o += (n_tb > 0 ? n_tb : 1);
     L.scal = o; o += 8;
     L.size = o;
     return L;
@@ -402,24 +499,31 @@ __device__ __forceinline__ void mixture(const Grp<G>& g, const DevMech& M, const
 
 // Net rate omega of every reaction at the clipped temperature (gpuReaction.H:472-488)
 // With write_cache, kf, 1/Kc and the third-body Ak of every reaction are kept
-// in kcache[] for the Jacobian at the same state (same T and concentrations,
-// hence the same values: the reference evaluates them twice).
+// for the Jacobian at the same state (same T and concentrations, hence the
+// same values: the reference evaluates them twice), in the reaction's own
+// staging slots 1..3 (every reaction has at least four: omega, dwdT and one
+// term per side); only the Jacobian's parameters overwrite them, after reading.
 template <int G, class W>
 __device__ __forceinline__ void stage_omega(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
                                             const TCache& tc, bool write_cache) {
     for (int q = g.lane; q < M.nR; q += G) {
+        // the reaction's table entries are requested together, ahead of use
         const int type = ldg(M.rtype + q);
+        const int irr = ldg(M.rirr + q);
+        const int so = ldg(M.slot + q);
+        const int tbr = ldg(M.tb_row + q);
+        const double Mc = tbr >= 0 ? w[L.Mtb + tbr] : 0.0;
         double dummy, Ak = 0.0;
-        const double kf = rate_k(M, q, type, tc, w, L.c, false, &dummy, &Ak);
+        const double kf = rate_k(M, q, type, tc, Mc, false, &dummy, &Ak);
         double kr = 0.0, invKc = 1.0;
-        if (!ldg(M.rirr + q)) {
+        if (!irr) {
             invKc = exp(-reaction_lnKc(M, q, tc, nullptr, nullptr));
             kr = kf * invKc;
         }
         if (write_cache) {
-            w[L.kcache + 3 * q] = kf;
-            w[L.kcache + 3 * q + 1] = invKc;
-            w[L.kcache + 3 * q + 2] = Ak;
+            w[L.stage + so + 1] = kf;
+            w[L.stage + so + 2] = invKc;
+            w[L.stage + so + 3] = Ak;
         }
         const int sp = ldg(M.sp_off + q);
         const int nl = ldg(M.nl + q), nr = ldg(M.nr + q);
@@ -428,9 +532,41 @@ __device__ __forceinline__ void stage_omega(const Grp<G>& g, const DevMech& M, c
             Cf *= specie_pow(w[L.c + ldg(M.sidx + sp + e)], ldg(M.siexp + sp + e), ldg(M.sexp + sp + e));
         for (int e = nl; e < nl + nr; ++e)
             Cr *= specie_pow(w[L.c + ldg(M.sidx + sp + e)], ldg(M.siexp + sp + e), ldg(M.sexp + sp + e));
-        w[L.stage + ldg(M.slot + q)] = kf * Cf - kr * Cr;
+        w[L.stage + so] = kf * Cf - kr * Cr;
     }
     g.sync();
+}
+
+__host__ __device__ constexpr int log2_group(int G) { return G <= 1 ? 0 : 1 + log2_group(G / 2); }
+
+// Runs this thread's share of a gather stream (gf_internal.h, Stream):
+// dst[pos] = sum of coef * src[slot] over each entry's records, in order.
+// Every record load is independent of the sums (coalesced 16-byte loads), so
+// they pipeline; one thread owns each output entry (no barriers inside).
+template <int G, class W>
+__device__ __forceinline__ void stream_gather(const Grp<G>& g, const Stream& st, const W& w, int src, int dst) {
+    constexpr int U = 8;  // records in flight per thread
+    const int4* r = reinterpret_cast<const int4*>(st.rec) + g.lane;
+    const int len = st.len;
+    double acc = 0.0;
+    for (int k0 = 0; k0 < len; k0 += U) {
+        int4 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = (k0 + u < len) ? __ldg(r + (size_t)(k0 + u) * G) : make_int4(-1, -1, 0, 0);
+        // the sources of the batch are read before any of its results is
+        // stored (the source and destination regions are disjoint)
+        double x[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) x[u] = v[u].y >= 0 ? w[src + v[u].y] : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (v[u].y >= 0) acc += __hiloint2double(v[u].w, v[u].z) * x[u];
+            if (v[u].x >= 0) {
+                w[dst + v[u].x] = acc;
+                acc = 0.0;
+            }
+        }
+    }
 }
 
 // dN_s/dt gathered in the reference's order, scaled to dY/dt (gpuODESystem.H:40-48,
@@ -439,12 +575,11 @@ template <int G, class W>
 __device__ __forceinline__ void gather_rhs(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
                                            int out_off, double rhoM, double CpM) {
     const int nS = M.nS;
+    stream_gather(g, M.dst[log2_group(G)], w, L.stage, out_off);
+    g.sync();
     double s_h = 0;
     for (int s = g.lane; s < nS; s += G) {
-        double acc = 0;
-        const int e1 = ldg(M.dn_ptr + s + 1);
-        for (int k = ldg(M.dn_ptr + s); k < e1; ++k) acc += ldg(M.dn_coef + k) * w[L.stage + ldg(M.dn_slot + k)];
-        acc *= ldg(M.W + s) / rhoM;
+        const double acc = w[out_off + s] * (ldg(M.W + s) / rhoM);
         w[out_off + s] = acc;
         s_h += acc * w[L.Ha + s];
     }
@@ -473,6 +608,10 @@ __device__ __forceinline__ void derivatives(const Grp<G>& g, const DevMech& M, c
     write_cache = write_cache && (Tc == T);
     {
         GF_PH_BEGIN(g)
+        if (M.n_tb > 0) {
+            third_body_all(g, M, w, L.c, L.Mtb);
+            g.sync();
+        }
         stage_omega(g, M, w, L, tc, write_cache);
         GF_PH_END(g, PH_OMEGA)
     }
@@ -482,6 +621,62 @@ __device__ __forceinline__ void derivatives(const Grp<G>& g, const DevMech& M, c
         gather_rhs(g, M, w, L, out_off, rhoM, CpM);
         GF_PH_END(g, PH_GATHER_RHS)
     }
+}
+
+// One side of a reaction (species entries b .. b+n of the stoichiometry):
+// returns C = prod c^e (calcCf / calcCr, gpuReaction.H:372-386) and writes
+// kmul * dC/dc_j to out + j, each the product over i of e_i c_i^(e_i - 1)
+// (i == j) or c_i^e_i (i != j) in the reference's order (calcdCfdcj /
+// calcdCrdcj, :388-470). Up to kInlineSide species the powers stay in
+// registers; wider sides recompute them (the same values).
+constexpr int kInlineSide = 4;
+template <class W>
+__device__ __forceinline__ double side_products(const DevMech& M, const W& w, int c_off, int b, int n, double kmul,
+                                                int out) {
+    if (n <= kInlineSide) {
+        double pw[kInlineSide], dm[kInlineSide];
+#pragma unroll
+        for (int e = 0; e < kInlineSide; ++e) {
+            pw[e] = 1.0;
+            dm[e] = 1.0;
+            if (e < n) {
+                const double x = w[c_off + ldg(M.sidx + b + e)];
+                const int ie = ldg(M.siexp + b + e);
+                const double se = ldg(M.sexp + b + e);
+                pw[e] = specie_pow(x, ie, se);
+                dm[e] = se * specie_pow_m1(x, ie, se);
+            }
+        }
+        double C = 1.0;
+#pragma unroll
+        for (int e = 0; e < kInlineSide; ++e)
+            if (e < n) C *= pw[e];
+#pragma unroll
+        for (int j = 0; j < kInlineSide; ++j) {
+            if (j < n) {
+                double d = 1;
+#pragma unroll
+                for (int i = 0; i < kInlineSide; ++i)
+                    if (i < n) d *= (i == j) ? dm[i] : pw[i];
+                w[out + j] = d * kmul;
+            }
+        }
+        return C;
+    }
+    double C = 1.0;
+    for (int e = 0; e < n; ++e)
+        C *= specie_pow(w[c_off + ldg(M.sidx + b + e)], ldg(M.siexp + b + e), ldg(M.sexp + b + e));
+    for (int j = 0; j < n; ++j) {
+        double d = 1;
+        for (int i = 0; i < n; ++i) {
+            const double x = w[c_off + ldg(M.sidx + b + i)];
+            const int ie = ldg(M.siexp + b + i);
+            const double se = ldg(M.sexp + b + i);
+            d *= (i == j) ? se * specie_pow_m1(x, ie, se) : specie_pow(x, ie, se);
+        }
+        w[out + j] = d * kmul;
+    }
+    return C;
 }
 
 // Per-reaction Jacobian parameters (computeReactionParameters, gpuReaction.H:650-702)
@@ -498,32 +693,16 @@ __device__ __forceinline__ void stage_jacobian_params(const Grp<G>& g, const Dev
         if (use_cache) {
             // dk/dT = k dln(k)/dT with the kInf factor for fall-off rates
             // (gpuFallOffReactionRate.H:140-141)
-            kf = w[L.kcache + 3 * q];
-            cachedInvKc = w[L.kcache + 3 * q + 1];
-            Ak = w[L.kcache + 3 * q + 2];
+            kf = w[L.stage + so + 1];
+            cachedInvKc = w[L.stage + so + 2];
+            Ak = w[L.stage + so + 3];
             const int f = (type == GF_RATE_LINDEMANN_FALLOFF || type == GF_RATE_TROE_FALLOFF) ? 1 : 0;
             ddT = kf * arr_dlnkdT(M, q, f, tc);
         } else {
-            kf = rate_k(M, q, type, tc, w, L.c, true, &ddT, &Ak);
+            const int tbr = ldg(M.tb_row + q);
+            kf = rate_k(M, q, type, tc, tbr >= 0 ? w[L.Mtb + tbr] : 0.0, true, &ddT, &Ak);
         }
-        double lp[kMaxW];
-        double Cf = 1.0;
-        for (int e = 0; e < nl; ++e) {
-            lp[e] = specie_pow(w[L.c + ldg(M.sidx + sp + e)], ldg(M.siexp + sp + e), ldg(M.sexp + sp + e));
-            Cf *= lp[e];
-        }
-        for (int j = 0; j < nl; ++j) {
-            double d = 1;
-            for (int i = 0; i < nl; ++i) {
-                if (i == j) {
-                    d *= ldg(M.sexp + sp + i) *
-                         specie_pow_m1(w[L.c + ldg(M.sidx + sp + i)], ldg(M.siexp + sp + i), ldg(M.sexp + sp + i));
-                } else {
-                    d *= lp[i];
-                }
-            }
-            w[L.stage + so + 2 + j] = d * kf;
-        }
+        const double Cf = side_products(M, w, L.c, sp, nl, kf, L.stage + so + 2);
         double dwdT = Cf * ddT;
         double omega = Cf * kf;
         double Cr = 0.0, invKc = 1.0;
@@ -539,48 +718,24 @@ __device__ __forceinline__ void stage_jacobian_params(const Grp<G>& g, const Dev
             }
             const double dKcdTbyKc = reaction_dKcdTbyKc(M, q, tc, Gstd, a);
             const double kr = kf * invKc;
-            double rp[kMaxW];
-            Cr = 1.0;
-            for (int e = 0; e < nr; ++e) {
-                rp[e] = specie_pow(w[L.c + ldg(M.sidx + sp + nl + e)], ldg(M.siexp + sp + nl + e),
-                                   ldg(M.sexp + sp + nl + e));
-                Cr *= rp[e];
-            }
+            Cr = side_products(M, w, L.c, sp + nl, nr, kr, L.stage + so + 2 + nl);
             const double dkrdT = ddT * invKc - kr * dKcdTbyKc;
             dwdT -= Cr * dkrdT;
             omega -= Cr * kr;
-            for (int j = 0; j < nr; ++j) {
-                double d = 1;
-                for (int i = 0; i < nr; ++i) {
-                    if (i == j) {
-                        const int b = sp + nl + i;
-                        d *= ldg(M.sexp + b) * specie_pow_m1(w[L.c + ldg(M.sidx + b)], ldg(M.siexp + b), ldg(M.sexp + b));
-                    } else {
-                        d *= rp[i];
-                    }
-                }
-                w[L.stage + so + 2 + nl + j] = d * kr;
-            }
         }
         w[L.stage + so] = omega;
         w[L.stage + so + 1] = dwdT;
-        if (type == GF_RATE_THIRD_BODY_ARRHENIUS) {
-            w[L.stage + so + 2 + nl + nr] = Ak;
-            w[L.stage + so + 3 + nl + nr] = Cf - Cr * invKc;
-        }
+        if (type == GF_RATE_THIRD_BODY_ARRHENIUS) w[L.stage + so + 2 + nl + nr] = Ak * (Cf - Cr * invKc);
     }
     g.sync();
 }
 
 // gpuODESystem::jacobian (gpuODESystem.H:198-281): dfdx (entries 0..nS) and J
 // (m x m, Y and T rows/columns; the p row/column are zero).
-//   phase 1 (lanes over rows): raw dN/dc and T-column pair contributions;
-//   phase 2 (lanes over columns): third-body dk/dc rows, reaction by reaction;
+//   raw entries (gather stream, one thread per entry): dN/dc, T-column and
+//     third-body terms in the reference's order per entry;
 //   phase 3 (lanes over rows): ddY_dcdY (gpuODESystem.H:65-103);
 //   then the T row (ddT_dtdY, ddT_dtdT, :108-146).
-// Within an entry the pair terms keep the reference's order; third-body terms
-// follow all pair terms of the entry (the reference interleaves them by
-// reaction), an ulp-level reordering.
 template <int G, class W>
 __device__ __forceinline__ void jacobian(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
                                          int y_off, double p, bool allow_cache = false) {
@@ -597,9 +752,15 @@ __device__ __forceinline__ void jacobian(const Grp<G>& g, const DevMech& M, cons
     const bool use_cache = allow_cache && w[L.scal + S_KCACHE_T] == tc.T;
     {
         GF_PH_BEGIN(g)
+        if (!use_cache && M.n_tb > 0) {
+            third_body_all(g, M, w, L.c, L.Mtb);
+            g.sync();
+        }
         stage_jacobian_params(g, M, w, L, tc, use_cache);
         GF_PH_END(g, PH_JPARAMS)
     }
+    // the staging slots that held the cache now hold the Jacobian terms
+    if (allow_cache && g.lane == 0) w[L.scal + S_KCACHE_T] = -1.0;
     {
         GF_PH_BEGIN(g)
         gather_rhs(g, M, w, L, L.dfdx, rhoM, CpM);
@@ -607,28 +768,10 @@ __device__ __forceinline__ void jacobian(const Grp<G>& g, const DevMech& M, cons
     }
     {
     GF_PH_BEGIN(g)
-    // phase 1
-    for (int s = g.lane; s < nS; s += G) {
-        const int row = L.J + s * ld;
-        for (int c = 0; c <= nS; ++c) w[row + c] = 0.0;
-        const int e1 = ldg(M.jr_ptr + s + 1);
-        for (int k = ldg(M.jr_ptr + s); k < e1; ++k) {
-            const JrRec rec = M.jr[k];
-            w[row + rec.col] += rec.coef * w[L.stage + rec.slot];
-        }
-    }
+    // raw dN/dc, T-column and third-body terms of every entry (species rows x
+    // species and T columns), one thread per entry, in the reference's order
+    stream_gather(g, M.jst[log2_group(G)], w, L.stage, L.J);
     g.sync();
-    // phase 2
-    for (int t = 0; t < M.n_tbt; ++t) {
-        const int q = ldg(M.tbt_q + t);
-        const int s = ldg(M.tbt_s + t);
-        const double cf = ldg(M.tbt_coef + t);
-        const int so = ldg(M.slot + q) + 2 + ldg(M.nl + q) + ldg(M.nr + q);
-        const double Ak = w[L.stage + so], tmp = w[L.stage + so + 1];
-        const double* e = M.eff + (size_t)ldg(M.tb_row + q) * nS;
-        for (int c = g.lane; c < nS; c += G) w[L.J + s * ld + c] += cf * ((ldg(e + c) * Ak) * tmp);
-        g.sync();
-    }
     // phase 3
     for (int s = g.lane; s < nS; s += G) {
         const double WiByrhoM = ldg(M.W + s) / rhoM;
@@ -757,57 +900,300 @@ __device__ __forceinline__ void lu_decompose(const Grp<G>& g, const W& w, int A,
 // ascending order; row exchanges move rows that have received the same
 // updates), so the factors are identical; the trailing matrix receives NB
 // updates per load/store instead of one.
+// Panel steps k0 .. k1-1 of the blocked LU (a group of at most one warp):
+// pivot search, row exchange, zero-pivot fix, column scaling and the update of
+// the panel's remaining columns.
+template <int G, class W>
+__device__ __forceinline__ void lu_panel(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv, int m, int k0,
+                                         int k1) {
+    for (int k = k0; k < k1; ++k) {
+        double best = -1.0;
+        int bi = -1;
+        for (int i = k + g.lane; i < m; i += G) {
+            const double t = w[vv + i] * fabs(w[A + i * ld + k]);
+            if (t >= best) {
+                best = t;
+                bi = i;
+            }
+        }
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(g.mask, best, o, G);
+            const int oi = __shfl_xor_sync(g.mask, bi, o, G);
+            if (ob > best || (ob == best && oi > bi)) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        const int iMax = bi < 0 ? 0 : bi;
+        if (iMax != k) {
+            for (int j = g.lane; j < m; j += G) {
+                const double t = w[A + k * ld + j];
+                w[A + k * ld + j] = w[A + iMax * ld + j];
+                w[A + iMax * ld + j] = t;
+            }
+        }
+        g.sync();
+        if (g.lane == 0) {
+            w.ip(piv + k) = iMax;
+            if (iMax != k) w[vv + iMax] = w[vv + k];
+            if (w[A + k * ld + k] == 0.0) w[A + k * ld + k] = kSmall;
+        }
+        g.sync();
+        if (k != m - 1) {
+            const double rDiag = 1.0 / w[A + k * ld + k];
+            for (int i = k + 1 + g.lane; i < m; i += G) {
+                const double lik = w[A + i * ld + k] * rDiag;
+                w[A + i * ld + k] = lik;
+                for (int j = k + 1; j < k1; ++j) w[A + i * ld + j] -= lik * w[A + k * ld + j];
+            }
+            g.sync();
+        }
+    }
+}
+
+// Panel steps k0 .. k1-1 with the panel held in registers (one full warp):
+// lane l holds panel rows k0 + l + 32 r (r < RP) and their row scalings.
+// Pivot search, the exchange of two panel rows, the column scaling and the
+// panel update run on registers and shuffles; the exchanges of the columns
+// outside the panel are left to lu_apply_swaps. Same operations, in the same
+// order per entry, as lu_panel. The pivots are stored to piv[]; the panel and
+// the updated row scalings are written back to A and vv.
+// Difference: when every candidate of a column is NaN, the reference exchanges
+// row k with row 0 (its iMax starts at 0); here no exchange is made (iMax = k).
+template <int RP, int NB, class W>
+__device__ __forceinline__ void lu_panel_reg(const Grp<32>& g, const W& w, int A, int ld, int piv, int vv, int m,
+                                             int k0, int k1) {
+    const int l = g.lane;
+    const int kb = k1 - k0;
+    double a[RP][NB];
+    double sv[RP];
+#pragma unroll
+    for (int r = 0; r < RP; ++r) {
+        const int p = k0 + l + 32 * r;
+#pragma unroll
+        for (int t = 0; t < NB; ++t) a[r][t] = (p < m && t < kb) ? w[A + p * ld + k0 + t] : 0.0;
+        sv[r] = p < m ? w[vv + p] : 0.0;
+    }
+#pragma unroll
+    for (int kk = 0; kk < NB; ++kk) {
+        if (kk >= kb) break;
+        const int k = k0 + kk;
+        // pivot search: the last row with the largest vv * |a| (ludecompose.H:57-63)
+        double best = -1.0;
+        int bi = -1;
+#pragma unroll
+        for (int r = 0; r < RP; ++r) {
+            const int p = k0 + l + 32 * r;
+            if (p >= k && p < m) {
+                const double t = sv[r] * fabs(a[r][kk]);
+                if (t >= best) {
+                    best = t;
+                    bi = p;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi > bi)) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        const int iMax = bi < 0 ? k : bi;
+        const int lk = (k - k0) & 31, rk = (k - k0) >> 5;
+        if (iMax != k) {
+            // exchange panel rows k and iMax; vv[iMax] = vv[k] (:71-78)
+            const int li = (iMax - k0) & 31, ri = (iMax - k0) >> 5;
+#pragma unroll
+            for (int t = 0; t < NB; ++t) {
+                double xk = a[0][t], xi = a[0][t];
+#pragma unroll
+                for (int r = 1; r < RP; ++r) {
+                    if (r == rk) xk = a[r][t];
+                    if (r == ri) xi = a[r][t];
+                }
+                const double vk = __shfl_sync(0xffffffffu, xk, lk);
+                const double vi = __shfl_sync(0xffffffffu, xi, li);
+#pragma unroll
+                for (int r = 0; r < RP; ++r) {
+                    if (l == lk && r == rk) a[r][t] = vi;
+                    if (l == li && r == ri) a[r][t] = vk;
+                }
+            }
+            double sk = sv[0];
+#pragma unroll
+            for (int r = 1; r < RP; ++r)
+                if (r == rk) sk = sv[r];
+            sk = __shfl_sync(0xffffffffu, sk, lk);
+#pragma unroll
+            for (int r = 0; r < RP; ++r)
+                if (l == li && r == ri) sv[r] = sk;
+        }
+        if (l == 0) w.ip(piv + k) = iMax;
+        // pivot row k of the panel, broadcast; a zero pivot becomes gpuSmall (:81)
+        double urow[NB];
+#pragma unroll
+        for (int t = 0; t < NB; ++t) {
+            double x = a[0][t];
+#pragma unroll
+            for (int r = 1; r < RP; ++r)
+                if (r == rk) x = a[r][t];
+            urow[t] = (t >= kk && t < kb) ? __shfl_sync(0xffffffffu, x, lk) : 0.0;
+        }
+        if (urow[kk] == 0.0) {
+            urow[kk] = kSmall;
+#pragma unroll
+            for (int r = 0; r < RP; ++r)
+                if (l == lk && r == rk) a[r][kk] = kSmall;
+        }
+        if (k != m - 1) {
+            const double rDiag = 1.0 / urow[kk];
+#pragma unroll
+            for (int r = 0; r < RP; ++r) {
+                const int p = k0 + l + 32 * r;
+                if (p > k && p < m) {
+                    const double lik = a[r][kk] * rDiag;
+                    a[r][kk] = lik;
+#pragma unroll
+                    for (int t = kk + 1; t < NB; ++t)
+                        if (t < kb) a[r][t] -= lik * urow[t];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RP; ++r) {
+        const int p = k0 + l + 32 * r;
+        if (p < m) {
+#pragma unroll
+            for (int t = 0; t < NB; ++t)
+                if (t < kb) w[A + p * ld + k0 + t] = a[r][t];
+            w[vv + p] = sv[r];
+        }
+    }
+}
+
+// The row exchanges of panel steps k0 .. k1-1 (pivots in piv[]) applied in
+// order to one column j outside the panel.
+template <class W>
+__device__ __forceinline__ void lu_apply_swaps(const W& w, int A, int ld, int piv, int k0, int k1, int j) {
+    for (int k = k0; k < k1; ++k) {
+        const int iMax = w.ip(piv + k);
+        if (iMax != k) {
+            const double t = w[A + k * ld + j];
+            w[A + k * ld + j] = w[A + iMax * ld + j];
+            w[A + iMax * ld + j] = t;
+        }
+    }
+}
+
+// Register-panel form of the blocked LU for a full warp or a multi-warp group
+// (m <= 64): warp 0 factors each panel in registers; every column outside the
+// panel takes the panel's row exchanges, then (columns right of the panel) its
+// U12 rows; then the trailing matrix is updated (lanes over columns, warps over
+// rows). Every entry receives its updates in k order, as in lu_decompose.
+template <int G, int NB, class W>
+__device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv,
+                                                      int m) {
+    constexpr int NWp = G > 32 ? G / 32 : 1;
+    const int wid = G > 32 ? (int)(threadIdx.x >> 5) : 0;
+    const int l = G > 32 ? (int)(threadIdx.x & 31) : g.lane;
+    for (int k0 = 0; k0 < m; ) {
+        const int kb = min(NB, m - k0);
+        const int k1 = k0 + kb;
+        if (wid == 0) {
+            Grp<32> g32;
+            lu_panel_reg<2, NB>(g32, w, A, ld, piv, vv, m, k0, k1);
+        }
+        g.sync();
+        // row exchanges outside the panel, and U12 of the columns right of it
+        for (int j = g.lane; j < m - kb; j += G) {
+            const int jj = j < k0 ? j : j + kb;
+            lu_apply_swaps(w, A, ld, piv, k0, k1, jj);
+            if (jj >= k1) {
+                double u[NB];
+#pragma unroll
+                for (int t = 0; t < NB; ++t) u[t] = t < kb ? w[A + (k0 + t) * ld + jj] : 0.0;
+#pragma unroll
+                for (int t = 1; t < NB; ++t) {
+                    if (t < kb) {
+                        double v = u[t];
+#pragma unroll
+                        for (int t2 = 0; t2 < t; ++t2) v -= w[A + (k0 + t) * ld + k0 + t2] * u[t2];
+                        u[t] = v;
+                        w[A + (k0 + t) * ld + jj] = v;
+                    }
+                }
+            }
+        }
+        g.sync();
+        if (k1 >= m) break;
+        for (int j = k1 + l; j < m; j += 32) {
+            double u[NB];
+#pragma unroll
+            for (int t = 0; t < NB; ++t) u[t] = t < kb ? w[A + (k0 + t) * ld + j] : 0.0;
+            for (int i = k1 + wid; i < m; i += NWp) {
+                double a = w[A + i * ld + j];
+#pragma unroll
+                for (int t = 0; t < NB; ++t)
+                    if (t < kb) a -= w[A + i * ld + k0 + t] * u[t];
+                w[A + i * ld + j] = a;
+            }
+        }
+        g.sync();
+        k0 = k1;
+    }
+}
+
 template <int G, int NB, class W>
 __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv,
                                                      int m) {
+    if constexpr (G > 32) {
+        // multi-warp group: warp 0 factors each panel; the U12 rows and the
+        // trailing matrix are updated by all warps (lanes over columns, warps
+        // over rows), each entry still receiving its updates in k order
+        constexpr int NWp = G / 32;
+        const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+        for (int k0 = 0; k0 < m; k0 += NB) {
+            const int kb = min(NB, m - k0);
+            const int k1 = k0 + kb;
+            if (wid == 0) {
+                Grp<32> g32;
+                lu_panel(g32, w, A, ld, piv, vv, m, k0, k1);
+            }
+            __syncthreads();
+            if (k1 >= m) break;
+            for (int j = k1 + g.lane; j < m; j += G) {
+                for (int t = 1; t < kb; ++t) {
+                    double v = w[A + (k0 + t) * ld + j];
+                    for (int t2 = 0; t2 < t; ++t2) v -= w[A + (k0 + t) * ld + k0 + t2] * w[A + (k0 + t2) * ld + j];
+                    w[A + (k0 + t) * ld + j] = v;
+                }
+            }
+            __syncthreads();
+            for (int j = k1 + l; j < m; j += 32) {
+                double u[NB];
+#pragma unroll
+                for (int t = 0; t < NB; ++t) u[t] = t < kb ? w[A + (k0 + t) * ld + j] : 0.0;
+                for (int i = k1 + wid; i < m; i += NWp) {
+                    double a = w[A + i * ld + j];
+#pragma unroll
+                    for (int t = 0; t < NB; ++t)
+                        if (t < kb) a -= w[A + i * ld + k0 + t] * u[t];
+                    w[A + i * ld + j] = a;
+                }
+            }
+            __syncthreads();
+        }
+    } else {
     for (int k0 = 0; k0 < m; k0 += NB) {
         const int kb = min(NB, m - k0);
         const int k1 = k0 + kb;
         // 1. panel: columns [k0, k1), rows [k0, m)
-        for (int k = k0; k < k1; ++k) {
-            double best = -1.0;
-            int bi = -1;
-            for (int i = k + g.lane; i < m; i += G) {
-                const double t = w[vv + i] * fabs(w[A + i * ld + k]);
-                if (t >= best) {
-                    best = t;
-                    bi = i;
-                }
-            }
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) {
-                const double ob = __shfl_xor_sync(g.mask, best, o, G);
-                const int oi = __shfl_xor_sync(g.mask, bi, o, G);
-                if (ob > best || (ob == best && oi > bi)) {
-                    best = ob;
-                    bi = oi;
-                }
-            }
-            const int iMax = bi < 0 ? 0 : bi;
-            if (iMax != k) {
-                for (int j = g.lane; j < m; j += G) {
-                    const double t = w[A + k * ld + j];
-                    w[A + k * ld + j] = w[A + iMax * ld + j];
-                    w[A + iMax * ld + j] = t;
-                }
-            }
-            g.sync();
-            if (g.lane == 0) {
-                w.ip(piv + k) = iMax;
-                if (iMax != k) w[vv + iMax] = w[vv + k];
-                if (w[A + k * ld + k] == 0.0) w[A + k * ld + k] = kSmall;
-            }
-            g.sync();
-            if (k != m - 1) {
-                const double rDiag = 1.0 / w[A + k * ld + k];
-                for (int i = k + 1 + g.lane; i < m; i += G) {
-                    const double lik = w[A + i * ld + k] * rDiag;
-                    w[A + i * ld + k] = lik;
-                    for (int j = k + 1; j < k1; ++j) w[A + i * ld + j] -= lik * w[A + k * ld + j];
-                }
-                g.sync();
-            }
-        }
+        lu_panel(g, w, A, ld, piv, vv, m, k0, k1);
         if (k1 >= m) break;
         // 2. U12: rows [k0, k1), columns [k1, m)
         for (int j = k1 + g.lane; j < m; j += G) {
@@ -831,6 +1217,7 @@ __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w
             }
         }
         g.sync();
+    }
     }
 }
 
@@ -891,10 +1278,13 @@ __device__ __forceinline__ void lu_perm(const Grp<G>& g, const W& w, int piv, in
 // LUBacksubstitute with the right-hand side in registers: lane l holds rows
 // l, l + G, ...; the pivot value of each step is broadcast by a shuffle, so
 // the substitution chain runs without shared-memory round trips or barriers.
-// Same subtraction order as lu_solve.
+// Same subtraction order as lu_solve; the backward step multiplies by the
+// reciprocal of the diagonal, rdiag[j] = 1 / U[j][j] (computed once per LU),
+// instead of dividing (ulp-level).
 constexpr int kRegRows = 160;
 template <int G, class W>
-__device__ __forceinline__ void lu_solve_reg(const Grp<G>& g, const W& w, int A, int ld, int perm, int m, int b) {
+__device__ __forceinline__ void lu_solve_reg(const Grp<G>& g, const W& w, int A, int ld, int perm, int rdiag, int m,
+                                             int b) {
     constexpr int R = kRegRows / G;
     GF_PH_BEGIN(g)
     double x[R];
@@ -926,7 +1316,7 @@ __device__ __forceinline__ void lu_solve_reg(const Grp<G>& g, const W& w, int A,
             const int lmax = min(G, m - t * G);
             for (int l = lmax - 1; l >= 0; --l) {
                 const int j = t * G + l;
-                const double xj = __shfl_sync(g.mask, x[t], l, G) / w[A + j * ld + j];
+                const double xj = __shfl_sync(g.mask, x[t], l, G) * w[rdiag + j];
                 if (g.lane == l) x[t] = xj;
 #pragma unroll
                 for (int u = 0; u <= t; ++u) {
@@ -945,12 +1335,78 @@ __device__ __forceinline__ void lu_solve_reg(const Grp<G>& g, const W& w, int A,
     GF_PH_END(g, PH_SOLVE)
 }
 
+// Register form for one full warp with R rows per lane (m <= 32 R): lane l
+// holds rows l + 32 u. The steps run in tiles of 32 with the step index
+// unrolled, so the shuffle source lane, the tile and the row predicates are
+// compile-time and the loads of later steps can be issued early (the loop
+// stores nothing). Same operations and order as lu_solve_reg.
+template <int R, class W>
+__device__ __forceinline__ void lu_solve_warp(const W& w, int A, int ld, int perm, int rdiag, int m, int b) {
+    const int lane = threadIdx.x & 31;
+    double x[R];
+    bool in[R];
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+        const int i = u * 32 + lane;
+        in[u] = i < m;
+        x[u] = in[u] ? w[b + w.ip(perm + i)] : 0.0;
+    }
+    // forward substitution with the unit lower factor, column by column
+#pragma unroll
+    for (int t = 0; t < R; ++t) {
+        if (32 * t >= m - 1) break;
+#pragma unroll
+        for (int l = 0; l < 32; ++l) {
+            const int j = 32 * t + l;
+            if (j >= m - 1) break;
+            const double bj = __shfl_sync(0xffffffffu, x[t], l);
+            if (lane > l && in[t]) x[t] -= w[A + (32 * t + lane) * ld + j] * bj;
+#pragma unroll
+            for (int u = t + 1; u < R; ++u)
+                if (in[u]) x[u] -= w[A + (32 * u + lane) * ld + j] * bj;
+        }
+    }
+    // backward substitution, descending columns, x_j = (...) * (1 / U[j][j])
+#pragma unroll
+    for (int t = R - 1; t >= 0; --t) {
+        if (32 * t >= m) continue;
+#pragma unroll
+        for (int l = 31; l >= 0; --l) {
+            const int j = 32 * t + l;
+            if (j >= m) continue;
+            const double xj = __shfl_sync(0xffffffffu, x[t], l) * w[rdiag + j];
+            if (lane == l) x[t] = xj;
+            if (lane < l) x[t] -= w[A + (32 * t + lane) * ld + j] * xj;
+#pragma unroll
+            for (int u = 0; u < t; ++u) x[u] -= w[A + (32 * u + lane) * ld + j] * xj;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+        if (in[u]) w[b + 32 * u + lane] = x[u];
+    __syncwarp();
+}
+
+// rdiag: 1 / diagonal of U, used by the register form (G >= 16).
 template <int G, class W>
-__device__ __forceinline__ void lu_solve_any(const Grp<G>& g, const W& w, int A, int ld, int piv, int perm, int m,
-                                             int b) {
-    if constexpr (G >= 16) {
+__device__ __forceinline__ void lu_solve_any(const Grp<G>& g, const W& w, int A, int ld, int piv, int perm, int rdiag,
+                                             int m, int b) {
+    if constexpr (G >= 32) {
+        // the substitution chain is sequential: one warp (the cell's warp, or
+        // warp 0 of a multi-warp group) runs it in registers
+        if (m <= 64) {
+            g.sync();
+            GF_PH_BEGIN(g)
+            if (G == 32 || threadIdx.x < 32) lu_solve_warp<2>(w, A, ld, perm, rdiag, m, b);
+            g.sync();
+            GF_PH_END(g, PH_SOLVE)
+            return;
+        }
+    }
+    if constexpr (G >= 16 && G <= 32) {
         if (m <= kRegRows) {
-            lu_solve_reg(g, w, A, ld, perm, m, b);
+            lu_solve_reg(g, w, A, ld, perm, rdiag, m, b);
             return;
         }
     }
@@ -1025,12 +1481,26 @@ __device__ __forceinline__ RosCoeffs ros_coeffs(int solver) {
     return c;
 }
 
+// Stage coefficients by (uniform) stage index: a_ij of the derivative points
+// (stages 1 and 2), c_ij of the right-hand sides and d_i.
+__device__ __forceinline__ double ros_a(const RosCoeffs& C, int i, int j) {
+    return i == 1 ? C.a21 : (j == 0 ? C.a31 : C.a32);
+}
+__device__ __forceinline__ double ros_c(const RosCoeffs& C, int i, int j) {
+    if (i == 1) return C.c21;
+    if (i == 2) return j == 0 ? C.c31 : C.c32;
+    return j == 0 ? C.c41 : (j == 1 ? C.c42 : C.c43);
+}
+__device__ __forceinline__ double ros_d(const RosCoeffs& C, int i) {
+    return i == 0 ? C.d1 : (i == 1 ? C.d2 : (i == 2 ? C.d3 : C.d4));
+}
+
 // One attempt solve(y0, dydx0, dx, y) of gpuRosenbrock12/23/34 (their
 // solve(y0, dydx0, dx, y, buffer)); returns the normalised error
 // (normaliseError.H:6-29; the p entry contributes 0). y0 is at y0_off, the
 // candidate is written to yt_off.
 template <int G, class W>
-__device__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
+__device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
                               const OdeParams& o, int y0_off, int yt_off, double p, double dx) {
     const int m = M.m;
     const int ld = L.ld;
@@ -1042,32 +1512,48 @@ __device__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, con
     }
     {
         GF_PH_BEGIN(g)
-        lu_decompose_blocked<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
+        bool done = false;
+        if constexpr (G >= 32) {
+            if (m <= 64) {
+                lu_decompose_regpanel<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
+                done = true;
+            }
+        }
+        if (!done) lu_decompose_blocked<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
         GF_PH_END(g, PH_LU)
     }
-    if (G >= 16) lu_perm(g, w, L.piv, L.perm, m);
-    for (int i = g.lane; i < m; i += G) w[L.k1 + i] = w[L.dydx0 + i] + dx * C.d1 * w[L.dfdx + i];
-    lu_solve_any(g, w, L.J, ld, L.piv, L.perm, m, L.k1);
-    for (int i = g.lane; i < m; i += G) w[yt_off + i] = w[y0_off + i] + C.a21 * w[L.k1 + i];
-    derivatives(g, M, w, L, yt_off, p, L.dydx);
-    for (int i = g.lane; i < m; i += G)
-        w[L.k2 + i] = w[L.dydx + i] + dx * C.d2 * w[L.dfdx + i] + C.c21 * w[L.k1 + i] / dx;
-    lu_solve_any(g, w, L.J, ld, L.piv, L.perm, m, L.k2);
-    if (C.s >= 3) {
-        if (C.s == 4) {
-            for (int i = g.lane; i < m; i += G)
-                w[yt_off + i] = w[y0_off + i] + C.a31 * w[L.k1 + i] + C.a32 * w[L.k2 + i];
+    if (G >= 16) {
+        // the row scaling vv is no longer needed: it holds 1 / U[i][i] from here
+        for (int i = g.lane; i < m; i += G) w[L.vv + i] = 1.0 / w[L.J + i * ld + i];
+        lu_perm(g, w, L.piv, L.perm, m);
+    }
+    // stages: k_i solves (I/(gamma dx) - J) k_i = f_i + dx d_i dfdx + sum_j c_ij k_j / dx,
+    // f_0 = f(y0), f_i = f(y0 + sum_j a_ij k_j) where the method takes a new
+    // derivative (stage 1; stage 2 of Rosenbrock34), else the previous one.
+    // One loop, so the solve and the derivative each have a single call site.
+#pragma unroll 1
+    for (int st = 0; st < C.s; ++st) {
+        const int ki = L.k1 + st * m;
+        if (st == 1 || (st == 2 && C.s == 4)) {
+            for (int i = g.lane; i < m; i += G) {
+                double v = w[y0_off + i];
+                for (int j = 0; j < st; ++j) v += ros_a(C, st, j) * w[L.k1 + j * m + i];
+                w[yt_off + i] = v;
+            }
             derivatives(g, M, w, L, yt_off, p, L.dydx);
         }
-        for (int i = g.lane; i < m; i += G)
-            w[L.k3 + i] = w[L.dydx + i] + dx * C.d3 * w[L.dfdx + i] + (C.c31 * w[L.k1 + i] + C.c32 * w[L.k2 + i]) / dx;
-        lu_solve_any(g, w, L.J, ld, L.piv, L.perm, m, L.k3);
-    }
-    if (C.s == 4) {
-        for (int i = g.lane; i < m; i += G)
-            w[L.k4 + i] = w[L.dydx + i] + dx * C.d4 * w[L.dfdx + i] +
-                          (C.c41 * w[L.k1 + i] + C.c42 * w[L.k2 + i] + C.c43 * w[L.k3 + i]) / dx;
-        lu_solve_any(g, w, L.J, ld, L.piv, L.perm, m, L.k4);
+        const int src = st == 0 ? L.dydx0 : L.dydx;
+        const double dd = dx * ros_d(C, st);
+        for (int i = g.lane; i < m; i += G) {
+            double v = w[src + i] + dd * w[L.dfdx + i];
+            if (st > 0) {
+                double cs = ros_c(C, st, 0) * w[L.k1 + i];
+                for (int j = 1; j < st; ++j) cs += ros_c(C, st, j) * w[L.k1 + j * m + i];
+                v += cs / dx;
+            }
+            w[ki + i] = v;
+        }
+        lu_solve_any(g, w, L.J, ld, L.piv, L.perm, L.vv, m, ki);
     }
     double emax = 0.0;
     for (int i = g.lane; i < m; i += G) {
@@ -1106,7 +1592,7 @@ struct CellResult {
 // gf_cell_status. maxSteps exhausted: dxTry is left unchanged (the reference
 // returns without writing it).
 template <int G, class W>
-__device__ int ode_solve(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const OdeParams& o,
+__device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const OdeParams& o,
                          const RosCoeffs& C, double xStart, double xEnd, int* y_off, int* yt_off, double p,
                          double* dxTry, int* accepted, int* attempts) {
     double step_dxTry = *dxTry;
@@ -1165,8 +1651,8 @@ __device__ __forceinline__ unsigned long long dbl_key(double v) {
 // computeYNew / computeRR epilogue (gpuKernelEvaluator.cu:84-96) fused:
 // RR, the min of deltaTChemNew before clamping, and the clamp.
 template <int G, class W>
-__device__ void process_cell(const Grp<G>& g, const DevMech& M, const W& w, const LaunchArgs& a, int cell) {
-    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots);
+__device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, const W& w, const LaunchArgs& a, int cell) {
+    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
     const int nS = M.nS, m = M.m;
     const double* yin = a.Y0 + (size_t)cell * a.ld_y;
     int y_off = L.y0, yt_off = L.yt;

@@ -102,6 +102,47 @@ struct DevBuf {
     }
 };
 
+// Gather streams (gf::Stream): entries with their (slot, coef) records in
+// summation order, split over G threads so that the record counts balance
+// (greedy, largest entry first), each thread's entries in ascending order,
+// interleaved record k of thread t at k * G + t, padded to the longest thread.
+// An entry without records still gets one (it writes zero).
+std::vector<gf::StreamRec> build_stream(const std::vector<std::vector<std::pair<int, double>>>& entries,
+                                        const std::vector<int>& pos, int G, int* len_out) {
+    const int nE = (int)entries.size();
+    std::vector<int> order(nE);
+    for (int e = 0; e < nE; ++e) order[e] = e;
+    auto cnt = [&](int e) { return std::max<int>(1, (int)entries[e].size()); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cnt(a) > cnt(b); });
+    std::vector<long long> load(G, 0);
+    std::vector<std::vector<int>> owned(G);
+    for (int e : order) {
+        int t = 0;
+        for (int u = 1; u < G; ++u)
+            if (load[u] < load[t]) t = u;
+        load[t] += cnt(e);
+        owned[t].push_back(e);
+    }
+    int len = 0;
+    for (int t = 0; t < G; ++t) len = std::max<int>(len, (int)load[t]);
+    std::vector<gf::StreamRec> rec((size_t)std::max(len, 1) * G, gf::StreamRec{-1, -1, 0.0});
+    for (int t = 0; t < G; ++t) {
+        std::sort(owned[t].begin(), owned[t].end());
+        int k = 0;
+        for (int e : owned[t]) {
+            const auto& R = entries[e];
+            if (R.empty()) {
+                rec[(size_t)k++ * G + t] = gf::StreamRec{pos[e], -1, 0.0};
+                continue;
+            }
+            for (size_t i = 0; i < R.size(); ++i)
+                rec[(size_t)k++ * G + t] = gf::StreamRec{i + 1 == R.size() ? pos[e] : -1, R[i].first, R[i].second};
+        }
+    }
+    *len_out = len;
+    return rec;
+}
+
 }  // namespace
 
 struct gf_mech {
@@ -336,21 +377,20 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
             }
         }
         sp_off[q + 1] = sp_off[q] + x.n_lhs + x.n_rhs;
-        slot[q + 1] = slot[q] + 2 + x.n_lhs + x.n_rhs + (x.rate_type == GF_RATE_THIRD_BODY_ARRHENIUS ? 2 : 0);
+        slot[q + 1] = slot[q] + 2 + x.n_lhs + x.n_rhs + (x.rate_type == GF_RATE_THIRD_BODY_ARRHENIUS ? 1 : 0);
     }
     const int n_slots = slot[nR];
     // per-species terms, built over reactions in mechanism order r
     std::vector<std::vector<std::pair<int, double>>> dn(nS);
-    std::vector<std::vector<JrRec>> jr(nS);
-    std::vector<int> tbt_q, tbt_s;
-    std::vector<double> tbt_coef;
+    const int nE = nS * (nS + 1);  // raw-Jacobian entries: species rows x (species + T) columns
+    std::vector<std::vector<std::pair<int, double>>> je(nE);
     for (int r = 0; r < nR; ++r) {
         const gf_reaction& x = d->reactions[r];
         const int so = slot[rof[r]];
         // dNdtByV (gpuReaction.H:490-508)
         for (int i = 0; i < x.n_lhs; ++i) dn[x.lhs[i].index].push_back({so, -x.lhs[i].stoich});
         for (int i = 0; i < x.n_rhs; ++i) dn[x.rhs[i].index].push_back({so, x.rhs[i].stoich});
-        auto add = [&](int s, int c, int sl, double cf) { jr[s].push_back(JrRec{c, sl, cf}); };
+        auto add = [&](int s, int c, int sl, double cf) { je[(size_t)s * (nS + 1) + c].push_back({sl, cf}); };
         // jac_dCfdcj_contribution (gpuReaction.H:547-569)
         for (int j = 0; j < x.n_lhs; ++j) {
             const int sj = x.lhs[j].index;
@@ -371,35 +411,23 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
         // jac_dCdC_contribution (:614-648): fall-off ddc is identically zero (kInf
         // has no concentration dependence, gpuFallOffReactionRate.H:143-153)
         if (x.rate_type == GF_RATE_THIRD_BODY_ARRHENIUS) {
-            for (int i = 0; i < x.n_lhs; ++i) {
-                tbt_q.push_back(rof[r]);
-                tbt_s.push_back(x.lhs[i].index);
-                tbt_coef.push_back(-x.lhs[i].stoich);
-            }
-            for (int i = 0; i < x.n_rhs; ++i) {
-                tbt_q.push_back(rof[r]);
-                tbt_s.push_back(x.rhs[i].index);
-                tbt_coef.push_back(x.rhs[i].stoich);
-            }
+            const int sp = so + 2 + x.n_lhs + x.n_rhs;  // Ak * (Cf - Cr/Kc)
+            for (int i = 0; i < x.n_lhs; ++i)
+                for (int c = 0; c < nS; ++c) add(x.lhs[i].index, c, sp, -x.lhs[i].stoich * x.efficiencies[c]);
+            for (int i = 0; i < x.n_rhs; ++i)
+                for (int c = 0; c < nS; ++c) add(x.rhs[i].index, c, sp, x.rhs[i].stoich * x.efficiencies[c]);
         }
     }
-    std::vector<int> dn_ptr(nS + 1, 0), dn_slot;
-    std::vector<double> dn_coef;
-    std::vector<int> jr_ptr(nS + 1, 0);
-    std::vector<JrRec> jr_all;
-    for (int s = 0; s < nS; ++s) {
-        for (auto& t : dn[s]) {
-            dn_slot.push_back(t.first);
-            dn_coef.push_back(t.second);
-        }
-        dn_ptr[s + 1] = (int)dn_slot.size();
-        jr_all.insert(jr_all.end(), jr[s].begin(), jr[s].end());
-        jr_ptr[s + 1] = (int)jr_all.size();
+    const int ldJ = (nS + 1) | 1;  // the workspace Jacobian row stride (make_layout)
+    std::vector<int> dn_pos(nS), je_pos(nE);
+    for (int s2 = 0; s2 < nS; ++s2) dn_pos[s2] = s2;
+    for (int e = 0; e < nE; ++e) je_pos[e] = (e / (nS + 1)) * ldJ + e % (nS + 1);
+    std::vector<std::vector<StreamRec>> dst_rec(kNumGroupSizes), jst_rec(kNumGroupSizes);
+    int dst_len[kNumGroupSizes], jst_len[kNumGroupSizes];
+    for (int k = 0; k < kNumGroupSizes; ++k) {
+        dst_rec[k] = build_stream(dn, dn_pos, 1 << k, &dst_len[k]);
+        jst_rec[k] = build_stream(je, je_pos, 1 << k, &jst_len[k]);
     }
-    const int n_tbt = (int)tbt_q.size();
-    std::vector<double> eff_t((size_t)nS * std::max(n_tb, 1), 0.0);
-    for (int t = 0; t < n_tb; ++t)
-        for (int i = 0; i < nS; ++i) eff_t[(size_t)i * n_tb + t] = eff[(size_t)t * nS + i];
     // keep every array non-empty
     if (eff.empty()) eff.push_back(0.0);
     if (sidx.empty()) {
@@ -407,16 +435,6 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
         siexp.push_back(0);
         sst.push_back(0.0);
         sexp.push_back(0.0);
-    }
-    if (dn_slot.empty()) {
-        dn_slot.push_back(0);
-        dn_coef.push_back(0.0);
-    }
-    if (jr_all.empty()) jr_all.push_back(JrRec{0, 0, 0.0});
-    if (tbt_q.empty()) {
-        tbt_q.push_back(0);
-        tbt_s.push_back(0);
-        tbt_coef.push_back(0.0);
     }
 
     // ---- one device allocation
@@ -426,10 +444,13 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
                  oSlot = b.add(slot), oRY = b.add(rY), oRnm = b.add(rnm), oRns = b.add(rnm_small), oRTc = b.add(rTc),
                  oRc = b.add(rcoef), oLA0 = b.add(lnA0), oSA0 = b.add(sA0), oB0 = b.add(beta0), oT0 = b.add(Ta0),
                  oLA1 = b.add(lnA1), oSA1 = b.add(sA1), oB1 = b.add(beta1), oT1 = b.add(Ta1), oTroe = b.add(troe),
-                 oTb = b.add(tb_row), oEff = b.add(eff), oEffT = b.add(eff_t), oSi = b.add(sidx), oSie = b.add(siexp), oSst = b.add(sst),
-                 oSe = b.add(sexp), oDnp = b.add(dn_ptr), oDns = b.add(dn_slot), oDnc = b.add(dn_coef),
-                 oJrp = b.add(jr_ptr), oJr = b.add(jr_all), oTbq = b.add(tbt_q), oTbs = b.add(tbt_s),
-                 oTbc = b.add(tbt_coef);
+                 oTb = b.add(tb_row), oEff = b.add(eff), oSi = b.add(sidx), oSie = b.add(siexp), oSst = b.add(sst),
+                 oSe = b.add(sexp);
+    size_t oDst[kNumGroupSizes], oJst[kNumGroupSizes];
+    for (int k = 0; k < kNumGroupSizes; ++k) {
+        oDst[k] = b.add(dst_rec[k]);
+        oJst[k] = b.add(jst_rec[k]);
+    }
     gf_mech* m = new (std::nothrow) gf_mech;
     if (!m) return GF_ERR_OUT_OF_MEMORY;
     cudaGetDevice(&m->device);
@@ -453,7 +474,6 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     D.m = nS + 1;
     D.n_slots = n_slots;
     D.n_tb = n_tb;
-    D.n_tbt = n_tbt;
     D.Tlow = Tlow;
     D.Thigh = Thigh;
     D.W = (const double*)P(oW);
@@ -482,19 +502,14 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     D.troe = (const double*)P(oTroe);
     D.tb_row = (const int*)P(oTb);
     D.eff = (const double*)P(oEff);
-    D.eff_t = (const double*)P(oEffT);
     D.sidx = (const int*)P(oSi);
     D.siexp = (const int*)P(oSie);
     D.sst = (const double*)P(oSst);
     D.sexp = (const double*)P(oSe);
-    D.dn_ptr = (const int*)P(oDnp);
-    D.dn_slot = (const int*)P(oDns);
-    D.dn_coef = (const double*)P(oDnc);
-    D.jr_ptr = (const int*)P(oJrp);
-    D.jr = (const JrRec*)P(oJr);
-    D.tbt_q = (const int*)P(oTbq);
-    D.tbt_s = (const int*)P(oTbs);
-    D.tbt_coef = (const double*)P(oTbc);
+    for (int k = 0; k < kNumGroupSizes; ++k) {
+        D.dst[k] = Stream{(const StreamRec*)P(oDst[k]), dst_len[k]};
+        D.jst[k] = Stream{(const StreamRec*)P(oJst[k]), jst_len[k]};
+    }
     *out = m;
     return GF_OK;
 }
@@ -534,9 +549,10 @@ int gf_solver_create(const gf_mech* const* mechs, int n_mechs, const gf_ode_inpu
     s->ode = gf::OdeParams{in->solver, in->absTol, in->relTol, in->maxSteps, in->safeScale, in->alphaInc,
                            in->alphaDec, in->minScale, in->maxScale};
     s->Treact = Treact;
-    // default launch: persistent, a warp per cell, workspace in shared memory
-    // when it fits (the autotuner refines this per mechanism)
-    s->cfg = gf_launch_config{1, 32, 1, 1, 0, 0};  // kind, G, shared, cells/CTA, CTAs/SM, registers
+    // default launch: persistent, two warps per cell (one cell per CTA),
+    // workspace in shared memory when it fits (the autotuner refines this per
+    // mechanism)
+    s->cfg = gf_launch_config{1, 64, 1, 1, 0, 0};  // kind, G, shared, cells/CTA, CTAs/SM, registers
     if ((size_t)s->max_ws_doubles * sizeof(double) > 227 * 1024) s->cfg.scratch_in_shared = 0;
     cudaError_t e = cudaMalloc(&s->queue, 8 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&s->queue_host, 8 * sizeof(unsigned long long));
@@ -566,7 +582,8 @@ int gf_solver_set_launch(gf_solver* s, const gf_launch_config* cfg) {
     if (cfg->kind != 0 && cfg->kind != 1) return GF_ERR_INVALID_ARGUMENT;
     if (cfg->kind == 1) {
         const int G = cfg->threads_per_cell;
-        if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) return GF_ERR_INVALID_ARGUMENT;
+        if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 128 && G != 256)
+            return GF_ERR_INVALID_ARGUMENT;
         if (cfg->register_budget != 0 && cfg->register_budget != 1) return GF_ERR_INVALID_ARGUMENT;
         if (cfg->scratch_in_shared && (size_t)s->max_ws_doubles * sizeof(double) > 227 * 1024)
             return GF_ERR_UNSUPPORTED;

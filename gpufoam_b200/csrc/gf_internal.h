@@ -12,12 +12,23 @@ namespace gf {
 constexpr int kMaxW = GF_MAX_REACTION_WIDTH;
 constexpr int kNoIntExp = 2147483647 / 10;  // gpuLabelMax: "not an integer exponent"
 
-// One raw-Jacobian contribution of a species row: J[row][col] += coef * stage[slot].
-struct __align__(16) JrRec {
-    int col;
+// One record of a gather stream: acc += coef * src[slot] (slot < 0: nothing);
+// pos >= 0 marks the last record of an output entry: dst[pos] = acc, acc = 0.
+struct __align__(16) StreamRec {
+    int pos;
     int slot;
     double coef;
 };
+
+// The records of a gather y[pos] = sum coef * x[slot], entry by entry in the
+// reference's summation order, split over G threads (entries balanced by
+// record count) and interleaved: record k of thread t is rec[k * G + t], so
+// a warp's loads are coalesced and every load is independent of the sums.
+struct Stream {
+    const StreamRec* rec;
+    int len;  // records per thread (padded)
+};
+constexpr int kNumGroupSizes = 9;  // G = 1, 2, 4, ..., 256: stream index log2(G)
 
 // Device-resident mechanism tables. All arrays are device pointers; the struct
 // itself is passed to kernels by value.
@@ -35,20 +46,19 @@ struct __align__(16) JrRec {
 //  * stoichiometry: compact CSR, sp_off[q] .. + nl[q] (lhs) + nr[q] (rhs)
 //  * staging slots of reaction q start at slot[q]:
 //      [0] omega, [1] dwdT, [2 .. 2+nl) dCf*kf, [2+nl .. 2+nl+nr) dCr*kr,
-//      third body only: [2+nl+nr] Ak, [3+nl+nr] (Cf - Cr/Kc)
-//  * dn_*: per species s, the (omega slot, signed stoich) terms of dN_s/dt in
-//    mechanism order (gpuReaction.H:490-508)
-//  * jr_*: per species row, the raw dN/dc and T-column contributions in the
-//    reference's update order (gpuReaction.H:547-612 over reactions in
-//    mechanism order)
-//  * tbt_*: the third-body dk/dc rows (gpuReaction.H:614-648): reaction q,
-//    species row s, signed stoich; row s gains coef * (eff[c] * Ak) * (Cf - Cr/Kc)
-//    in every species column c.
+//      third body only: [2+nl+nr] Ak * (Cf - Cr/Kc)
+//  * dst[log2 G]: the gather streams of dN_s/dt: per species s the (omega slot,
+//    signed stoich) terms in mechanism order (gpuReaction.H:490-508)
+//  * jst[log2 G]: the gather streams of the raw Jacobian: entry (row s,
+//    column c < nS or the T column c = nS), position s * ld + c in the
+//    workspace Jacobian, takes its dN/dc, T-column and third-body terms in the
+//    reference's update order (gpuReaction.H:547-648 over reactions in
+//    mechanism order). A third-body term is (stoich * eff_c) * (Ak * (Cf -
+//    Cr/Kc)) (the reference: stoich * ((eff_c * Ak) * (Cf - Cr/Kc))).
 struct DevMech {
     int nS, nR, m;
     int n_slots;
     int n_tb;
-    int n_tbt;
     double Tlow, Thigh;        // reaction temperature limits (uniform)
     // species
     const double* W;
@@ -78,19 +88,12 @@ struct DevMech {
     const double* troe;        // [nR][4]: alpha, 1/Tsss, 1/Ts, Tss
     const int* tb_row;         // [nR] row of eff, -1 for plain Arrhenius
     const double* eff;         // [n_tb][nS]
-    const double* eff_t;       // [nS][n_tb] (species-major: coalesced across reactions)
     const int* sidx;
     const int* siexp;          // integer exponent or kNoIntExp
     const double* sst;
     const double* sexp;
-    const int* dn_ptr;         // [nS + 1]
-    const int* dn_slot;
-    const double* dn_coef;
-    const int* jr_ptr;         // [nS + 1]
-    const JrRec* jr;
-    const int* tbt_q;
-    const int* tbt_s;
-    const double* tbt_coef;
+    Stream dst[kNumGroupSizes];
+    Stream jst[kNumGroupSizes];
 };
 
 struct OdeParams {
@@ -103,7 +106,7 @@ struct OdeParams {
 // Per-cell workspace layout (in doubles) for a mechanism.
 struct WsLayout {
     int ld;          // Jacobian / LU row stride (odd, bank-conflict free columns)
-    int J, y0, yt, dydx0, dydx, dfdx, k1, k2, k3, k4, c, Cp, Ha, rhoMbyW, vj, vv, piv, perm, kcache, stage, scal;
+    int J, y0, yt, dydx0, dydx, dfdx, k1, k2, k3, k4, c, Cp, Ha, rhoMbyW, vj, vv, piv, perm, stage, Mtb, scal;
     int size;        // total doubles
 };
 

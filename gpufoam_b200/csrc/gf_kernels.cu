@@ -4,9 +4,10 @@
 //                        scratch interleaved in HBM: the reference's launch model
 //                        (for_each_index.H:25-48, singleCellSolver.H:27-51) with
 //                        coalesced scratch.
-//  * persistent_kernel — one CTA set sized to the SMs; groups of G threads pull
-//                        cells from an atomic work queue, scratch in shared memory
-//                        (or HBM), mixed mechanisms by per-cell id.
+//  * persistent_kernel — gf_persist.cuh (instantiated in gf_persist_g*.cu): one
+//                        CTA set sized to the SMs; groups of G threads (1..256)
+//                        pull cells from an atomic work queue, scratch in shared
+//                        memory (or HBM), mixed mechanisms by per-cell id.
 //  * rates / jacobian / lu / lusolve kernels — the parity entry points.
 #include <cuda_runtime.h>
 
@@ -15,20 +16,9 @@
 
 #include "gf_device.cuh"
 #include "gf_internal.h"
+#include "gf_persist.cuh"
 
 namespace gf {
-
-constexpr int kMaxMechs = 4;
-
-struct MechSet {
-    DevMech m[kMaxMechs];
-    int n;
-};
-
-__device__ __forceinline__ const DevMech& pick(const MechSet& P, const LaunchArgs& a, long long cell) {
-    const int id = a.mech_id ? a.mech_id[cell] : 0;
-    return P.m[id];
-}
 
 // ------------------------------------------------------------ solve kernels
 
@@ -39,32 +29,6 @@ __global__ void __launch_bounds__(128) plain_kernel(const MechSet P, const Launc
     const DevMech& M = pick(P, a, cell);
     WsS w{a.ws + cell, a.ws_slot_stride};
     process_cell(g, M, w, a, (int)cell);
-}
-
-// MINB = 1: up to 255 registers per thread (fewer resident groups, no spills);
-// MINB = 4: at most 128 registers (more resident groups).
-template <int G, bool SHARED, int MINB>
-__global__ void __launch_bounds__(128, MINB) persistent_kernel(const MechSet P, const LaunchArgs a, int ws_per_cell,
-                                                               long long n_slots) {
-    extern __shared__ double smem[];
-    Grp<G> g;
-    const int gpb = blockDim.x / G;
-    const int gib = threadIdx.x / G;
-    const long long slot = (long long)blockIdx.x * gpb + gib;
-    for (;;) {
-        long long cell = 0;
-        if (g.lane == 0) cell = (long long)atomicAdd(a.queue, 1ull);
-        cell = g.bcast_ll(cell, 0);
-        if (cell >= a.n_cells) break;
-        const DevMech& M = pick(P, a, cell);
-        if (SHARED) {
-            process_cell(g, M, WsC{smem + (size_t)gib * ws_per_cell}, a, (int)cell);
-        } else if (G == 1) {
-            process_cell(g, M, WsS{a.ws + slot, n_slots}, a, (int)cell);
-        } else {
-            process_cell(g, M, WsC{a.ws + slot * ws_per_cell}, a, (int)cell);
-        }
-    }
 }
 
 __global__ void reset_kernel(unsigned long long* q) {
@@ -80,7 +44,7 @@ __global__ void reset_kernel(unsigned long long* q) {
 __global__ void __launch_bounds__(32) rates_kernel(const DevMech M, const double* y, double* dydx) {
     extern __shared__ double smem[];
     Grp<32> g;
-    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots);
+    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
     const int n = M.nS + 2;
     const double* yi = y + (size_t)blockIdx.x * n;
     WsC w{smem};
@@ -95,7 +59,7 @@ __global__ void __launch_bounds__(32) rates_kernel(const DevMech M, const double
 __global__ void __launch_bounds__(32) jacobian_kernel(const DevMech M, const double* y, double* dfdx, double* J) {
     extern __shared__ double smem[];
     Grp<32> g;
-    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots);
+    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
     const int n = M.nS + 2;
     const double* yi = y + (size_t)blockIdx.x * n;
     WsC w{smem};
@@ -145,7 +109,7 @@ __global__ void __launch_bounds__(32) lusolve_kernel(int m, const double* LU, co
 
 // ---------------------------------------------------------------- launchers
 
-WsLayout ws_layout(const DevMech& m) { return make_layout(m.nS, m.nR, m.n_slots); }
+WsLayout ws_layout(const DevMech& m) { return make_layout(m.nS, m.nR, m.n_slots, m.n_tb); }
 
 int device_sm_count() {
     int dev = 0, n = 0;
@@ -154,20 +118,17 @@ int device_sm_count() {
     return n;
 }
 
-template <int G, bool SHARED>
-static const void* persistent_ptr(int slim) {
-    return slim ? reinterpret_cast<const void*>(&persistent_kernel<G, SHARED, 4>)
-                : reinterpret_cast<const void*>(&persistent_kernel<G, SHARED, 1>);
-}
-
 static const void* persistent_fn(int G, bool shared, int slim) {
     switch (G) {
-    case 1: return shared ? persistent_ptr<1, true>(slim) : persistent_ptr<1, false>(slim);
-    case 2: return shared ? persistent_ptr<2, true>(slim) : persistent_ptr<2, false>(slim);
-    case 4: return shared ? persistent_ptr<4, true>(slim) : persistent_ptr<4, false>(slim);
-    case 8: return shared ? persistent_ptr<8, true>(slim) : persistent_ptr<8, false>(slim);
-    case 16: return shared ? persistent_ptr<16, true>(slim) : persistent_ptr<16, false>(slim);
-    case 32: return shared ? persistent_ptr<32, true>(slim) : persistent_ptr<32, false>(slim);
+    case 1: return persistent_fn_g1(shared, slim);
+    case 2: return persistent_fn_g2(shared, slim);
+    case 4: return persistent_fn_g4(shared, slim);
+    case 8: return persistent_fn_g8(shared, slim);
+    case 16: return persistent_fn_g16(shared, slim);
+    case 32: return persistent_fn_g32(shared, slim);
+    case 64: return persistent_fn_g64(shared, slim);
+    case 128: return persistent_fn_g128(shared, slim);
+    case 256: return persistent_fn_g256(shared, slim);
     default: return nullptr;
     }
 }
@@ -177,9 +138,10 @@ int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* 
     const bool shared = cfg.scratch_in_shared != 0;
     const void* fn = persistent_fn(G, shared, cfg.register_budget);
     if (!fn) return -1;
-    int cpb = cfg.cells_per_block > 0 ? cfg.cells_per_block : std::max(1, 128 / G);
+    // G <= 32: several groups per CTA of at most 128 threads; G > 32: one group
+    int cpb = G > 32 ? 1 : (cfg.cells_per_block > 0 ? cfg.cells_per_block : std::max(1, 128 / G));
     int threads = cpb * G;
-    if (threads > 128) {
+    if (G <= 32 && threads > 128) {
         cpb = 128 / G;
         threads = cpb * G;
     }
@@ -191,6 +153,15 @@ int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* 
         if (smem > 227 * 1024) return -2;
     }
     if (shared) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // shared-memory carveout: by default as much as the resident CTAs can use;
+    // with blocks_per_sm set, just enough for those CTAs, so that the rest of
+    // the SM's 256 KB serves as L1 for the mechanism tables
+    int carve = 100;
+    if (cfg.blocks_per_sm > 0) {
+        const size_t need = (size_t)cfg.blocks_per_sm * (smem + 1024) + 1024;
+        carve = (int)std::min<size_t>(100, (need * 100 + 228 * 1024 - 1) / (228 * 1024));
+    }
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) return -3;
     if (per_sm <= 0) return -4;
@@ -267,14 +238,21 @@ int launch_lusolve(int n_mats, int m, const double* LU, const int* piv, double* 
 
 #ifdef GF_PHASE_TIMERS
 }  // namespace gf
+// Phase-timer cycles summed over every kernel translation unit (profiling
+// builds only).
 extern "C" int gf_debug_phase_cycles(unsigned long long* out, int reset) {
-    using gf::g_phase_cycles;
-    cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(unsigned long long) * 16);
-    if (reset) {
-        unsigned long long z[16] = {};
-        cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
-    }
-    return (int)cudaGetLastError();
+    using namespace gf;
+    for (int i = 0; i < 16; ++i) out[i] = 0;
+    phase_cycles_local(out, reset);
+    phase_cycles_g1(out, reset);
+    phase_cycles_g2(out, reset);
+    phase_cycles_g4(out, reset);
+    phase_cycles_g8(out, reset);
+    phase_cycles_g16(out, reset);
+    phase_cycles_g32(out, reset);
+    phase_cycles_g64(out, reset);
+    phase_cycles_g128(out, reset);
+    return phase_cycles_g256(out, reset);
 }
 namespace gf {
 #endif

@@ -1,0 +1,96 @@
+// The persistent work-queue solve kernel (sm_100a), shared by the per-G
+// instantiation files gf_persist_g*.cu (one translation unit per group size,
+// so that the variants compile in parallel).
+//
+// CTAs sized to the SMs; groups of G threads pull cells from an atomic work
+// queue until it is empty. G <= 32: several groups per CTA (at most 128
+// threads); G = 64, 128, 256: one group (one cell at a time) per CTA. The
+// per-cell workspace lives in shared memory (SHARED) or in an HBM slot per
+// resident group. Mixed mechanisms are selected by the per-cell id.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gf_device.cuh"
+#include "gf_internal.h"
+
+namespace gf {
+
+constexpr int kMaxMechs = 4;
+
+struct MechSet {
+    DevMech m[kMaxMechs];
+    int n;
+};
+
+__device__ __forceinline__ const DevMech& pick(const MechSet& P, const LaunchArgs& a, long long cell) {
+    const int id = a.mech_id ? a.mech_id[cell] : 0;
+    return P.m[id];
+}
+
+// threads per CTA the kernel is compiled for
+template <int G>
+struct PersistShape {
+    static constexpr int kThreads = G > 128 ? G : 128;
+    // SLIM = 1: at most 128 registers per thread (512 resident threads per SM)
+    static constexpr int kMinBlocksSlim = 512 / kThreads;
+};
+
+template <int G, bool SHARED, int SLIM>
+__global__ void __launch_bounds__(PersistShape<G>::kThreads, SLIM ? PersistShape<G>::kMinBlocksSlim : 1)
+    persistent_kernel(const MechSet P, const LaunchArgs a, int ws_per_cell, long long n_slots) {
+    extern __shared__ double smem[];
+    Grp<G> g;
+    const int gpb = G > 32 ? 1 : blockDim.x / G;
+    const int gib = G > 32 ? 0 : threadIdx.x / G;
+    const long long slot = (long long)blockIdx.x * gpb + gib;
+    for (;;) {
+        long long cell = 0;
+        if (g.lane == 0) cell = (long long)atomicAdd(a.queue, 1ull);
+        cell = g.bcast_ll(cell, 0);
+        if (cell >= a.n_cells) break;
+        const DevMech& M = pick(P, a, cell);
+        if (SHARED) {
+            process_cell(g, M, WsC{smem + (size_t)gib * ws_per_cell}, a, (int)cell);
+        } else if (G == 1) {
+            process_cell(g, M, WsS{a.ws + slot, n_slots}, a, (int)cell);
+        } else {
+            process_cell(g, M, WsC{a.ws + slot * ws_per_cell}, a, (int)cell);
+        }
+    }
+}
+
+template <int G>
+const void* persistent_variant(bool shared, int slim) {
+    if (shared)
+        return slim ? reinterpret_cast<const void*>(&persistent_kernel<G, true, 1>)
+                    : reinterpret_cast<const void*>(&persistent_kernel<G, true, 0>);
+    return slim ? reinterpret_cast<const void*>(&persistent_kernel<G, false, 1>)
+                : reinterpret_cast<const void*>(&persistent_kernel<G, false, 0>);
+}
+
+// defined in gf_persist_g<G>.cu
+const void* persistent_fn_g1(bool shared, int slim);
+const void* persistent_fn_g2(bool shared, int slim);
+const void* persistent_fn_g4(bool shared, int slim);
+const void* persistent_fn_g8(bool shared, int slim);
+const void* persistent_fn_g16(bool shared, int slim);
+const void* persistent_fn_g32(bool shared, int slim);
+const void* persistent_fn_g64(bool shared, int slim);
+const void* persistent_fn_g128(bool shared, int slim);
+const void* persistent_fn_g256(bool shared, int slim);
+
+#ifdef GF_PHASE_TIMERS
+// phase-timer accumulators of the gf_persist_g<G>.cu units (profiling builds)
+int phase_cycles_g1(unsigned long long* out, int reset);
+int phase_cycles_g2(unsigned long long* out, int reset);
+int phase_cycles_g4(unsigned long long* out, int reset);
+int phase_cycles_g8(unsigned long long* out, int reset);
+int phase_cycles_g16(unsigned long long* out, int reset);
+int phase_cycles_g32(unsigned long long* out, int reset);
+int phase_cycles_g64(unsigned long long* out, int reset);
+int phase_cycles_g128(unsigned long long* out, int reset);
+int phase_cycles_g256(unsigned long long* out, int reset);
+#endif
+
+}  // namespace gf

@@ -140,9 +140,11 @@ typedef struct gf_ode_inputs {
  * cells, the reference's launch model); 1 = persistent work queue. */
 typedef struct gf_launch_config {
     int kind;
-    int threads_per_cell;    /* 1, 2, 4, 8, 16 or 32 (persistent only)          */
+    int threads_per_cell;    /* persistent only: 1, 2, 4, 8, 16, 32 (groups inside a
+                                warp) or 64, 128, 256 (one cell per CTA)         */
     int scratch_in_shared;   /* 1: per-cell workspace in shared memory           */
-    int cells_per_block;     /* groups per CTA (persistent only; CTAs have at most 128 threads) */
+    int cells_per_block;     /* groups per CTA (persistent, threads_per_cell <= 32;
+                                CTAs have at most 128 threads)                   */
     int blocks_per_sm;       /* 0 = as many as fit                               */
     int register_budget;     /* persistent only: 0 = up to 255 registers per thread,
                                 1 = at most 128 (more resident cell groups)      */

@@ -27,6 +27,10 @@ LAUNCHES = {
     "persist-g32-smem": dict(kind=1, threads_per_cell=32, scratch_in_shared=1),
     "persist-g32-hbm": dict(kind=1, threads_per_cell=32, scratch_in_shared=0),
     "persist-g4-hbm": dict(kind=1, threads_per_cell=4, scratch_in_shared=0),
+    "persist-g64-smem": dict(kind=1, threads_per_cell=64, scratch_in_shared=1),
+    "persist-g128-smem-slim": dict(kind=1, threads_per_cell=128, scratch_in_shared=1, register_budget=1),
+    "persist-g256-smem": dict(kind=1, threads_per_cell=256, scratch_in_shared=1),
+    "persist-g128-hbm": dict(kind=1, threads_per_cell=128, scratch_in_shared=0),
 }
 
 
@@ -103,7 +107,7 @@ def test_cells_vs_golden(torch, name, solver):
 
 @pytest.mark.parametrize("launch", list(LAUNCHES))
 def test_launch_forms_agree_with_oracle(torch, launch):
-    """Every launch form (plain, persistent G=1..32, shared / HBM scratch)
+    """Every launch form (plain, persistent G=1..256, shared / HBM scratch)
     against the oracle on 192 H2-size cells, R34."""
     raw = M.h2_size(0)
     mech = E.Mechanism(raw)
@@ -122,7 +126,7 @@ def test_grisize_cells_vs_oracle(torch):
     mech = E.Mechanism(raw)
     cells = M.make_cells(raw, 48, seed=31)
     ref = Oracle(raw, "port").cells(ode_inputs(23), cells, 1e-6, 1e-7)
-    for launch in ("persist-g32-smem", "plain"):
+    for launch in ("persist-g32-smem", "persist-g128-smem-slim", "plain"):
         Y, dtc, cnt, st, _ = run_cells(torch, mech, cells, 1e-6, 1e-7, 23, LAUNCHES[launch])
         assert (st == 0).all()
         assert_states_close(Y, ref[0], raw.n_species, 1e-4, launch)
