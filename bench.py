@@ -46,9 +46,17 @@ WORKLOADS = {
     "h2-1k": dict(mech="h2", n=1024, dT=1e-5, T=(1000.0, 2500.0)),
     "gri-100k": dict(mech="gri", n=100_000, dT=1e-6, T=(1000.0, 2500.0)),
     "gri-bimodal-1M": dict(mech="gri", n=1_000_000, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0))),
+    # one launch over three mechanisms (10, 53 and 100 species), per-cell
+    # deltaT ~ log-U[1e-7, 1e-4] s and p ~ U[0.5, 40] atm, cells shuffled
+    "mixed-750k": dict(mixed=((("h2", 200_000), ("gri", 500_000), ("large", 50_000))), dT=0.0,
+                       dT_cell=(1e-7, 1e-4), p=(0.5 * 101325.0, 40 * 101325.0)),
+    # the same proportions at a tenth of the size (a bounded measurement)
+    "mixed-75k": dict(mixed=((("h2", 20_000), ("gri", 50_000), ("large", 5_000))), dT=0.0,
+                      dT_cell=(1e-7, 1e-4), p=(0.5 * 101325.0, 40 * 101325.0)),
     # small cases of the same kernels, for ncu captures and launch sweeps
     "gri-4k": dict(mech="gri", n=4096, dT=1e-6, T=(1000.0, 2500.0)),
     "gri-16k": dict(mech="gri", n=16384, dT=1e-6, T=(1000.0, 2500.0)),
+    "gri-bimodal-64k": dict(mech="gri", n=65536, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0))),
 }
 DTC0 = 1e-7
 
@@ -75,14 +83,42 @@ def parse():
     return ap.parse_args()
 
 
-def make_batch(wl, seed):
+class Batch:
+    """A workload's cells: mechanisms, states [n][ld], per-cell mechanism ids
+    and time steps (None for a single mechanism / one deltaT)."""
+
+    def __init__(self, raws, cells, mech_id=None, dT_cell=None):
+        self.raws, self.cells, self.mech_id, self.dT_cell = raws, cells, mech_id, dT_cell
+
+
+def _mech(name):
     from gpufoam_b200 import mechanism as M
-    raw = M.h2_size(0) if wl["mech"] == "h2" else M.gri_size(0)
+    return {"h2": M.h2_size, "gri": M.gri_size, "large": M.large}[name](0)
+
+
+def make_batch(wl, seed) -> Batch:
+    from gpufoam_b200 import mechanism as M
+    if "mixed" in wl:
+        rng = np.random.default_rng(seed)
+        raws = [_mech(name) for name, _ in wl["mixed"]]
+        ld = max(r.n_eqns for r in raws)
+        n = sum(k for _, k in wl["mixed"])
+        cells = np.zeros((n, ld))
+        mid = np.empty(n, dtype=np.int32)
+        o = 0
+        for k, ((_, cnt), r) in enumerate(zip(wl["mixed"], raws)):
+            cells[o:o + cnt, :r.n_eqns] = M.make_cells(r, cnt, seed=seed + 17 * k, p_range=wl["p"])
+            mid[o:o + cnt] = k
+            o += cnt
+        perm = rng.permutation(n)
+        dts = M.log_uniform(rng, wl["dT_cell"][0], wl["dT_cell"][1], n)
+        return Batch(raws, np.ascontiguousarray(cells[perm]), mid[perm], dts)
+    raw = _mech(wl["mech"])
     if "bimodal" in wl:
         cells = M.make_cells(raw, wl["n"], seed=seed, bimodal=wl["bimodal"])
     else:
         cells = M.make_cells(raw, wl["n"], seed=seed, T_range=wl["T"])
-    return raw, cells
+    return Batch([raw], cells)
 
 
 class Clocks:
@@ -126,9 +162,7 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference_rate(raw, cells, solver, dT, seconds, nthreads):
-    """The reference's own singleCellSolver (oracle/_ref) over a bounded
-    sample of cells with all host threads; returns (cells/s, sample size, kind)."""
+def _cpu_rate_one(raw, cells, solver, dT, dT_cell, seconds, nthreads):
     from oracle.oracle import REF_LIB, Oracle, ode_inputs
     kind = "reference" if os.path.exists(REF_LIB) else "port"
     o = Oracle(raw, kind)
@@ -136,16 +170,36 @@ def cpu_reference_rate(raw, cells, solver, dT, seconds, nthreads):
     n = max(nthreads * 4, 32)
     done, t_total = 0, 0.0
     while t_total < seconds and done < cells.shape[0]:
-        chunk = cells[done:done + n]
+        chunk = np.ascontiguousarray(cells[done:done + n, :raw.n_eqns])
         t0 = time.perf_counter()
-        if kind == "reference":
+        if kind == "reference" and dT_cell is None:
             o.cells_uncounted(inp, chunk, dT, DTC0, nthreads=nthreads)
         else:
-            o.cells(inp, chunk, dT, DTC0, nthreads=nthreads)
+            o.cells(inp, chunk, dT, DTC0, deltaT_cell=None if dT_cell is None else dT_cell[done:done + n],
+                    nthreads=nthreads)
         t_total += time.perf_counter() - t0
         done += chunk.shape[0]
         n = min(n * 2, 4096)
     return done / t_total, done, kind, t_total
+
+
+def cpu_reference_rate(batch, solver, dT, seconds, nthreads, offset=0):
+    """The reference's own singleCellSolver (oracle/_ref, or the port) over a
+    bounded sample of the batch with all host threads. Several mechanisms: each
+    is timed on its own cells for a share of the time, and the batch rate is
+    n / sum_k(n_k / rate_k). Returns (cells/s, sample size, kind, seconds)."""
+    if batch.mech_id is None:
+        return _cpu_rate_one(batch.raws[0], batch.cells[offset:], solver, dT, None, seconds, nthreads)
+    n = batch.cells.shape[0]
+    t_inv, done_all, t_all, kind = 0.0, 0, 0.0, None
+    for k, raw in enumerate(batch.raws):
+        sel = np.nonzero(batch.mech_id == k)[0]
+        share = max(seconds * len(sel) / n, seconds / (2 * len(batch.raws)))
+        r, done, kind, t = _cpu_rate_one(raw, batch.cells[sel], solver, dT, batch.dT_cell[sel], share, nthreads)
+        t_inv += len(sel) / r
+        done_all += done
+        t_all += t
+    return n / t_inv, done_all, kind, t_all
 
 
 def main():
@@ -155,17 +209,17 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nthreads = os.cpu_count() or 1
+    cfg_desc = {"workload": args.workload, "solver": f"Rosenbrock{args.solver}", "relTol": 1e-4, "absTol": 1e-8,
+                "deltaT": wl["dT"] if "dT_cell" not in wl else f"per cell, log-U{list(wl['dT_cell'])} s"}
 
     if args.impl == "reference":
         if rank != 0:
             return
-        raw, cells = make_batch(wl, seed=1000)
-        times = []
-        sample = None
-        rates = []
+        batch = make_batch(wl, seed=1000)
+        times, rates, sample = [], [], None
         for k in range(args.warmup + args.steps):
-            r, done, kind, t = cpu_reference_rate(raw, cells[(k * 997) % max(1, cells.shape[0] - 4096):], args.solver,
-                                                  wl["dT"], max(2.0, args.cpu_seconds / 4), nthreads)
+            r, done, kind, t = cpu_reference_rate(batch, args.solver, wl["dT"], max(2.0, args.cpu_seconds / 4),
+                                                  nthreads, offset=(k * 997) % max(1, batch.cells.shape[0] - 4096))
             if k >= args.warmup:
                 rates.append(r)
                 times.append(t)
@@ -175,8 +229,7 @@ def main():
                 "value": value, "unit": "cells/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": args.workload, "cells": wl["n"], "deltaT": wl["dT"],
-                           "solver": f"Rosenbrock{args.solver}", "relTol": 1e-4, "absTol": 1e-8},
+                "config": dict(cfg_desc, cells=int(batch.cells.shape[0])),
                 "cpu_baseline": {"value": value, "unit": "cells/s", "cores": nthreads, "kind": kind,
                                  "sample": f"{sample} cells of the {args.workload} batch per step, OpenMP "
                                            f"schedule(dynamic,64) over cells"},
@@ -195,22 +248,25 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    raw, cells = make_batch(wl, seed=1000 + rank)
+    batch = make_batch(wl, seed=1000 + rank)
+    cells = batch.cells
     n = cells.shape[0]
-    mech = E.Mechanism(raw)
+    mechs = [E.Mechanism(r) for r in batch.raws]
     ode = E.OdeInputs(f"Rosenbrock{args.solver}", absTol=1e-8, relTol=1e-4)
     Y0 = torch.as_tensor(cells, device="cuda")
+    mid = None if batch.mech_id is None else torch.as_tensor(batch.mech_id, device="cuda")
+    dtcell = None if batch.dT_cell is None else torch.as_tensor(batch.dT_cell, device="cuda")
     dtc0 = torch.full((n,), DTC0, dtype=torch.float64, device="cuda")
     dtc = dtc0.clone()
     Ynew = torch.empty_like(Y0)
-    counters = torch.empty((n, 2), dtype=torch.int32, device="cuda")
     lib = N.load()
 
     def timed(solver, steps, warmup):
         stream = torch.cuda.current_stream()
         for _ in range(warmup):
             dtc.copy_(dtc0)
-            solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, want_status=False, want_counters=False, want_stats=False)
+            solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, deltaT_cell=dtcell, mech_id=mid, want_status=False,
+                         want_counters=False, want_stats=False)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -220,8 +276,8 @@ def main():
             dtc.copy_(dtc0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            out = solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, want_status=False, want_counters=True,
-                               want_stats=False)
+            out = solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, deltaT_cell=dtcell, mech_id=mid, want_status=False,
+                               want_counters=True, want_stats=False)
             e1.record(stream)
             launches += 2  # queue reset + the solve kernel
             if world > 1:
@@ -236,24 +292,32 @@ def main():
         cnt = out["counters"].cpu().numpy()
         return ms, cnt, launches
 
+    def flop_of(cnt):
+        if batch.mech_id is None:
+            return F.total(batch.raws[0], args.solver, int(cnt[:, 1].sum()), int(cnt[:, 0].sum()))
+        return sum(F.total(r, args.solver, int(cnt[batch.mech_id == k, 1].sum()), int(cnt[batch.mech_id == k, 0].sum()))
+                   for k, r in enumerate(batch.raws))
+
     # FP64 roofline denominator, measured on this GPU
     import ctypes
     peak = ctypes.c_double()
     N.check(lib.gf_measure_fp64_peak(200.0, ctypes.byref(peak)), "gf_measure_fp64_peak")
 
-    solver = E.Solver([mech], ode)
+    solver = E.Solver(mechs, ode)
     solver.set_launch(kind=1, threads_per_cell=args.threads_per_cell, scratch_in_shared=args.shared,
                       register_budget=args.register_budget)
     tuned = None
     if args.launch != "fixed":
         from gpufoam_b200 import autotune
         rng = np.random.default_rng(7)
-        sample = cells[rng.choice(n, size=min(n, 8192), replace=False)]
-        tuned = autotune.tune(solver, sample, wl["dT"], DTC0, use_cache=(args.launch == "auto"),
+        pick = rng.choice(n, size=min(n, 8192), replace=False)
+        tuned = autotune.tune(solver, cells[pick], wl["dT"], DTC0, use_cache=(args.launch == "auto"),
+                              deltaT_cell=None if dtcell is None else dtcell[torch.as_tensor(pick, device="cuda")],
+                              mech_id=None if mid is None else mid[torch.as_tensor(pick, device="cuda")],
                               verbose=False)
         if args.launch == "sweep" and rank == 0:
             for cfg, ms in tuned["table"]:
-                print(json.dumps({"sweep": cfg, "ms": ms, "cells": int(sample.shape[0])}), file=sys.stderr)
+                print(json.dumps({"sweep": cfg, "ms": ms, "cells": int(len(pick))}), file=sys.stderr)
     clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
     ms, cnt, launches = timed(solver, args.steps, args.warmup)
     clk = clocks.stop() if clocks else None
@@ -265,12 +329,12 @@ def main():
         t_max = float(t.item())
     value = world * n / (t_max * 1e-3)
     attempts, accepted = int(cnt[:, 1].sum()), int(cnt[:, 0].sum())
-    flop = F.total(raw, args.solver, attempts, accepted)
+    flop = flop_of(cnt)
     achieved = flop / (ms_step * 1e-3) / 1e12
 
     plain = None
     if not args.no_plain:
-        ps = E.Solver([mech], ode)
+        ps = E.Solver(mechs, ode)
         ps.set_launch(kind=0)
         pms, pcnt, _ = timed(ps, max(1, min(args.steps, 2)), 1)
         pm = float(np.mean(pms))
@@ -283,8 +347,9 @@ def main():
         del ps
 
     e2e = None
-    if not args.no_e2e:
-        ev = E.GpuKernelEvaluator(n, raw.n_eqns, raw.n_species, mech, ode)
+    if not args.no_e2e and batch.mech_id is None:
+        raw = batch.raws[0]
+        ev = E.GpuKernelEvaluator(n, raw.n_eqns, raw.n_species, mechs[0], ode)
         ev.solver.set_launch(**solver.get_launch())
         hY = torch.empty((n, raw.n_eqns), dtype=torch.float64, pin_memory=True)
         hY.copy_(torch.as_tensor(cells))
@@ -311,12 +376,44 @@ def main():
                "d2h_bytes_per_step": int(n * (raw.n_species + 1) * 8),
                "api": "GpuKernelEvaluator.computeRR -> gf_compute_rr (pinned host arrays)"}
         del ev
+    elif not args.no_e2e:
+        # several mechanisms: the device-memory entry point from pinned host arrays
+        hY = torch.empty(cells.shape, dtype=torch.float64, pin_memory=True)
+        hY.copy_(torch.as_tensor(cells))
+        hm = torch.as_tensor(batch.mech_id).pin_memory()
+        hdt = torch.as_tensor(batch.dT_cell).pin_memory()
+        hdtc = torch.full((n,), DTC0, dtype=torch.float64).pin_memory()
+        hout = torch.empty(cells.shape, dtype=torch.float64, pin_memory=True)
+        hdtn = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        em = []
+        for _ in range(max(1, min(args.steps, 2))):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dY, dm, ddt, dd = (hY.to("cuda", non_blocking=True), hm.to("cuda", non_blocking=True),
+                               hdt.to("cuda", non_blocking=True), hdtc.to("cuda", non_blocking=True))
+            solver.solve(dY, 0.0, dd, Ynew=dY, deltaT_cell=ddt, mech_id=dm, want_status=False,
+                         want_counters=False, want_stats=False)
+            hout.copy_(dY, non_blocking=True)
+            hdtn.copy_(dd, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+            em.append(e0.elapsed_time(e1))
+        et = float(np.mean(em))
+        if world > 1:
+            t = torch.tensor([et], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            et = float(t.item())
+        e2e = {"value": world * n / (et * 1e-3), "unit": "cells/s",
+               "h2d_bytes_per_step": int(n * (cells.shape[1] * 8 + 4 + 8 + 8)),
+               "d2h_bytes_per_step": int(n * (cells.shape[1] + 1) * 8),
+               "api": "Solver.solve -> gf_solve with per-cell deltaT and mechanism id (pinned host arrays)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r, done, kind, t = cpu_reference_rate(raw, cells, args.solver, wl["dT"], args.cpu_seconds, nthreads)
+        r, done, kind, t = cpu_reference_rate(batch, args.solver, wl["dT"], args.cpu_seconds, nthreads)
         cpu = {"value": r, "unit": "cells/s", "cores": nthreads, "kind": kind,
-               "sample": f"first {done} cells of the {args.workload} batch ({t:.1f} s), the reference's "
+               "sample": f"{done} cells of the {args.workload} batch ({t:.1f} s), the reference's "
                          f"singleCellSolver per cell, OpenMP schedule(dynamic,64)"}
 
     if rank == 0:
@@ -325,11 +422,10 @@ def main():
             "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "cells_per_gpu": n, "species": raw.n_species,
-                       "reactions": raw.n_reactions, "deltaT": wl["dT"], "deltaTChem0": DTC0,
-                       "solver": f"Rosenbrock{args.solver}", "relTol": 1e-4, "absTol": 1e-8,
-                       "launch": solver.get_launch(), "l2": "inputs larger than L2 (not flushed)",
-                       "parallelism": f"cells sharded over {world} GPU(s)"},
+            "config": dict(cfg_desc, cells_per_gpu=n,
+                           mechanisms=[f"{r.n_species} species / {r.n_reactions} reactions" for r in batch.raws],
+                           deltaTChem0=DTC0, launch=solver.get_launch(), l2="inputs larger than L2 (not flushed)",
+                           parallelism=f"cells sharded over {world} GPU(s)"),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value, "traffic": None,
                          "peak_source": "measured DFMA microbenchmark on this GPU (gf_measure_fp64_peak)",

@@ -190,6 +190,62 @@ __device__ __forceinline__ Poly7 species_coeffs(const DevMech& M, int i, double 
     return a;
 }
 
+// A reaction's packed data (RxnHead) and the species entries of both sides,
+// requested with independent 16-byte loads before any of them is used.
+struct Rxn {
+    int type, irr, slot, tb_row, nl, nr, sp_off, nm_small;
+    double lnA0, beta0, Ta0, sA0, Tcommon, Y, nm;
+    int idx[2][kSideInline], iexp[2][kSideInline];
+    double sexp[2][kSideInline];
+};
+
+__device__ __forceinline__ void load_rxn(const DevMech& M, int q, Rxn& R) {
+    const int4* h = reinterpret_cast<const int4*>(M.rxh + q);
+    const int4 h0 = __ldg(h), h1 = __ldg(h + 1);
+    const double2* hd = reinterpret_cast<const double2*>(M.rxh + q) + 2;
+    const double2 d0 = __ldg(hd), d1 = __ldg(hd + 1);
+    const int4* sp = reinterpret_cast<const int4*>(M.rxs + (size_t)q * 2 * kSideInline);
+    int4 v[2 * kSideInline];
+#pragma unroll
+    for (int e = 0; e < 2 * kSideInline; ++e) v[e] = __ldg(sp + e);
+    R.type = h0.x;
+    R.irr = h0.y;
+    R.slot = h0.z;
+    R.tb_row = h0.w;
+    R.nl = h1.x;
+    R.nr = h1.y;
+    R.sp_off = h1.z;
+    R.nm_small = h1.w;
+    R.lnA0 = d0.x;
+    R.beta0 = d0.y;
+    R.Ta0 = d1.x;
+    R.sA0 = d1.y;
+    const double2 d2 = __ldg(hd + 2);
+    R.Tcommon = d2.x;
+    R.Y = d2.y;
+    R.nm = __ldg(reinterpret_cast<const double*>(hd + 3));
+#pragma unroll
+    for (int e = 0; e < 2 * kSideInline; ++e) {
+        R.idx[e / kSideInline][e % kSideInline] = v[e].x;
+        R.iexp[e / kSideInline][e % kSideInline] = v[e].y;
+        R.sexp[e / kSideInline][e % kSideInline] = __hiloint2double(v[e].w, v[e].z);
+    }
+}
+
+__device__ __forceinline__ Poly7 reaction_coeffs_at(const DevMech& M, int r, double T, double Tcommon) {
+    const int b = coef_branch(T, Tcommon);
+    const double* c = M.rcoef + (size_t)b * 7 * M.nR + r;
+    Poly7 a;
+    a.a0 = ldg(c);
+    a.a1 = ldg(c + M.nR);
+    a.a2 = ldg(c + 2 * M.nR);
+    a.a3 = ldg(c + 3 * M.nR);
+    a.a4 = ldg(c + 4 * M.nR);
+    a.a5 = ldg(c + 5 * M.nR);
+    a.a6 = ldg(c + 6 * M.nR);
+    return a;
+}
+
 __device__ __forceinline__ Poly7 reaction_coeffs(const DevMech& M, int r, double T) {
     const int b = coef_branch(T, ldg(M.rTcommon + r));
     const double* c = M.rcoef + (size_t)b * 7 * M.nR + r;
@@ -253,25 +309,23 @@ __device__ __forceinline__ TCache make_tcache(double T) {
 }
 
 // ln of the K part of Kc, capped as K() caps it (gpuThermo.H:84-85)
-__device__ __forceinline__ double reaction_lnKc(const DevMech& M, int q, const TCache& tc, double* Gstd_out,
-                                                Poly7* a_out) {
-    const Poly7 a = reaction_coeffs(M, q, tc.T);
-    const double Y = ldg(M.rY + q);
+__device__ __forceinline__ double reaction_lnKc(const DevMech& M, int q, const Rxn& R, const TCache& tc,
+                                                double* Gstd_out, Poly7* a_out) {
+    const Poly7 a = reaction_coeffs_at(M, q, tc.T, R.Tcommon);
     const double Gstd = th_Gstd(a, tc.T, tc.logT);
-    const double arg = -Y * Gstd * tc.invT * (1.0 / kRR);
+    const double arg = -R.Y * Gstd * tc.invT * (1.0 / kRR);
     double lnK = arg < 600 ? arg : 0.5 * log(kVGreat);
-    if (!ldg(M.rnm_small + q)) lnK += ldg(M.rnm + q) * tc.lx;
+    if (!R.nm_small) lnK += R.nm * tc.lx;
     if (Gstd_out) *Gstd_out = Gstd;
     if (a_out) *a_out = a;
     return lnK;
 }
 
 // dKc/dT / Kc (gpuThermo.H:160-166)
-__device__ __forceinline__ double reaction_dKcdTbyKc(const DevMech& M, int q, const TCache& tc, double Gstd,
-                                                     const Poly7& a) {
+__device__ __forceinline__ double reaction_dKcdTbyKc(const Rxn& R, const TCache& tc, double Gstd, const Poly7& a) {
     const double S = th_S_pstd(a, tc.T, tc.logT);
-    double ret = (S + Gstd * tc.invT) * ldg(M.rY + q) * tc.invT * (1.0 / kRR);
-    if (!ldg(M.rnm_small + q)) ret = ret - ldg(M.rnm + q) * tc.invT;
+    double ret = (S + Gstd * tc.invT) * R.Y * tc.invT * (1.0 / kRR);
+    if (!R.nm_small) ret = ret - R.nm * tc.invT;
     return ret;
 }
 
@@ -297,17 +351,19 @@ __device__ __forceinline__ double specie_pow_m1(double x, int iexp, double sexp)
     return iexp != kNoIntExp ? integer_pow(x, iexp - 1) : pow(x, sexp + (-1.0));
 }
 
-// ln|k| of Arrhenius factor f (0: k / k0, 1: kInf) and its sign
-__device__ __forceinline__ double arr_ln(const DevMech& M, int q, int f, const TCache& tc) {
-    const double lnA = ldg((f ? M.lnA1 : M.lnA0) + q);
-    const double beta = ldg((f ? M.beta1 : M.beta0) + q);
-    const double Ta = ldg((f ? M.Ta1 : M.Ta0) + q);
-    return fma(beta, tc.logT, lnA) - Ta * tc.invT;
+// ln|k| of an Arrhenius factor: k (or the fall-off k0) from the reaction's
+// head, kInf from the fall-off tables; and dln(k)/dT = (beta + Ta/T)/T
+__device__ __forceinline__ double arr_ln0(const Rxn& R, const TCache& tc) {
+    return fma(R.beta0, tc.logT, R.lnA0) - R.Ta0 * tc.invT;
 }
-__device__ __forceinline__ double arr_dlnkdT(const DevMech& M, int q, int f, const TCache& tc) {
-    const double beta = ldg((f ? M.beta1 : M.beta0) + q);
-    const double Ta = ldg((f ? M.Ta1 : M.Ta0) + q);
-    return (beta + Ta * tc.invT) * tc.invT;  // (beta + Ta/T)/T
+__device__ __forceinline__ double arr_ln1(const DevMech& M, int q, const TCache& tc) {
+    return fma(ldg(M.beta1 + q), tc.logT, ldg(M.lnA1 + q)) - ldg(M.Ta1 + q) * tc.invT;
+}
+__device__ __forceinline__ double arr_dlnkdT0(const Rxn& R, const TCache& tc) {
+    return (R.beta0 + R.Ta0 * tc.invT) * tc.invT;
+}
+__device__ __forceinline__ double arr_dlnkdT1(const DevMech& M, int q, const TCache& tc) {
+    return (ldg(M.beta1 + q) + ldg(M.Ta1 + q) * tc.invT) * tc.invT;
 }
 
 // Third-body concentrations M_t = sum_i eff_ti c_i of every third-body and
@@ -392,27 +448,28 @@ __device__ __forceinline__ double troe_F(const DevMech& M, int q, const TCache& 
 // gpuThirdBodyArrheniusReactionRate.H:105-121, gpuFallOffReactionRate.H:127-158).
 // Mc: the reaction's third-body concentration (third_body_all), unused for
 // plain Arrhenius rates.
-__device__ __forceinline__ double rate_k(const DevMech& M, int q, int type, const TCache& tc, double Mc,
+__device__ __forceinline__ double rate_k(const DevMech& M, int q, const Rxn& R, const TCache& tc, double Mc,
                                          bool want_dT, double* dT_out, double* Ak_out) {
+    const int type = R.type;
     if (type == GF_RATE_ARRHENIUS) {
-        const double Ak = ldg(M.sA0 + q) * exp(arr_ln(M, q, 0, tc));
-        if (want_dT) *dT_out = Ak * arr_dlnkdT(M, q, 0, tc);
+        const double Ak = R.sA0 * exp(arr_ln0(R, tc));
+        if (want_dT) *dT_out = Ak * arr_dlnkdT0(R, tc);
         return Ak;
     }
     if (type == GF_RATE_THIRD_BODY_ARRHENIUS) {
-        const double Ak = ldg(M.sA0 + q) * exp(arr_ln(M, q, 0, tc));
-        if (want_dT) *dT_out = Mc * (Ak * arr_dlnkdT(M, q, 0, tc));
+        const double Ak = R.sA0 * exp(arr_ln0(R, tc));
+        if (want_dT) *dT_out = Mc * (Ak * arr_dlnkdT0(R, tc));
         *Ak_out = Ak;
         return Mc * Ak;
     }
     // fall-off: Pr = k0 / kInf * M, k = kInf Pr / (1 + Pr) F
-    const double l0 = arr_ln(M, q, 0, tc), l1 = arr_ln(M, q, 1, tc);
-    const double s0 = ldg(M.sA0 + q), s1 = ldg(M.sA1 + q);
+    const double l0 = arr_ln0(R, tc), l1 = arr_ln1(M, q, tc);
+    const double s0 = R.sA0, s1 = ldg(M.sA1 + q);
     const double kInf = s1 * exp(l1);
     const double Pr = (s0 * s1) * exp(l0 - l1) * Mc;
     const double F = type == GF_RATE_TROE_FALLOFF ? troe_F(M, q, tc, Pr) : 1.0;
     const double temp = (Pr / (1.0 + Pr)) * F;
-    if (want_dT) *dT_out = (kInf * arr_dlnkdT(M, q, 1, tc)) * temp;
+    if (want_dT) *dT_out = (kInf * arr_dlnkdT1(M, q, tc)) * temp;
     return kInf * temp;
 }
 
@@ -507,17 +564,15 @@ template <int G, class W>
 __device__ __forceinline__ void stage_omega(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
                                             const TCache& tc, bool write_cache) {
     for (int q = g.lane; q < M.nR; q += G) {
-        // the reaction's table entries are requested together, ahead of use
-        const int type = ldg(M.rtype + q);
-        const int irr = ldg(M.rirr + q);
-        const int so = ldg(M.slot + q);
-        const int tbr = ldg(M.tb_row + q);
-        const double Mc = tbr >= 0 ? w[L.Mtb + tbr] : 0.0;
+        Rxn R;
+        load_rxn(M, q, R);
+        const int so = R.slot;
+        const double Mc = R.tb_row >= 0 ? w[L.Mtb + R.tb_row] : 0.0;
         double dummy, Ak = 0.0;
-        const double kf = rate_k(M, q, type, tc, Mc, false, &dummy, &Ak);
+        const double kf = rate_k(M, q, R, tc, Mc, false, &dummy, &Ak);
         double kr = 0.0, invKc = 1.0;
-        if (!irr) {
-            invKc = exp(-reaction_lnKc(M, q, tc, nullptr, nullptr));
+        if (!R.irr) {
+            invKc = exp(-reaction_lnKc(M, q, R, tc, nullptr, nullptr));
             kr = kf * invKc;
         }
         if (write_cache) {
@@ -525,13 +580,8 @@ __device__ __forceinline__ void stage_omega(const Grp<G>& g, const DevMech& M, c
             w[L.stage + so + 2] = invKc;
             w[L.stage + so + 3] = Ak;
         }
-        const int sp = ldg(M.sp_off + q);
-        const int nl = ldg(M.nl + q), nr = ldg(M.nr + q);
-        double Cf = 1.0, Cr = 1.0;
-        for (int e = 0; e < nl; ++e)
-            Cf *= specie_pow(w[L.c + ldg(M.sidx + sp + e)], ldg(M.siexp + sp + e), ldg(M.sexp + sp + e));
-        for (int e = nl; e < nl + nr; ++e)
-            Cr *= specie_pow(w[L.c + ldg(M.sidx + sp + e)], ldg(M.siexp + sp + e), ldg(M.sexp + sp + e));
+        const double Cf = side_C(M, w, L.c, R, 0);
+        const double Cr = side_C(M, w, L.c, R, 1);
         w[L.stage + so] = kf * Cf - kr * Cr;
     }
     g.sync();
@@ -623,46 +673,62 @@ __device__ __forceinline__ void derivatives(const Grp<G>& g, const DevMech& M, c
     }
 }
 
-// One side of a reaction (species entries b .. b+n of the stoichiometry):
-// returns C = prod c^e (calcCf / calcCr, gpuReaction.H:372-386) and writes
-// kmul * dC/dc_j to out + j, each the product over i of e_i c_i^(e_i - 1)
-// (i == j) or c_i^e_i (i != j) in the reference's order (calcdCfdcj /
-// calcdCrdcj, :388-470). Up to kInlineSide species the powers stay in
-// registers; wider sides recompute them (the same values).
-constexpr int kInlineSide = 4;
+// Product C = prod c^e of one side of a reaction (side 0: lhs, 1: rhs), in
+// the reference's order (calcCf / calcCr, gpuReaction.H:372-386).
 template <class W>
-__device__ __forceinline__ double side_products(const DevMech& M, const W& w, int c_off, int b, int n, double kmul,
-                                                int out) {
-    if (n <= kInlineSide) {
-        double pw[kInlineSide], dm[kInlineSide];
+__device__ __forceinline__ double side_C(const DevMech& M, const W& w, int c_off, const Rxn& R, int side) {
+    const int n = side ? R.nr : R.nl;
+    double C = 1.0;
+    if (n <= kSideInline) {
 #pragma unroll
-        for (int e = 0; e < kInlineSide; ++e) {
+        for (int e = 0; e < kSideInline; ++e)
+            if (e < n) C *= specie_pow(w[c_off + R.idx[side][e]], R.iexp[side][e], R.sexp[side][e]);
+        return C;
+    }
+    const int b = R.sp_off + (side ? R.nl : 0);
+    for (int e = 0; e < n; ++e)
+        C *= specie_pow(w[c_off + ldg(M.sidx + b + e)], ldg(M.siexp + b + e), ldg(M.sexp + b + e));
+    return C;
+}
+
+// One side of a reaction: returns C = prod c^e and writes kmul * dC/dc_j to
+// out + j, each the product over i of e_i c_i^(e_i - 1) (i == j) or c_i^e_i
+// (i != j) in the reference's order (calcdCfdcj / calcdCrdcj, :388-470). Up to
+// kSideInline species the powers stay in registers; wider sides recompute
+// them (the same values).
+template <class W>
+__device__ __forceinline__ double side_products(const DevMech& M, const W& w, int c_off, const Rxn& R, int side,
+                                                double kmul, int out) {
+    const int n = side ? R.nr : R.nl;
+    if (n <= kSideInline) {
+        double pw[kSideInline], dm[kSideInline];
+#pragma unroll
+        for (int e = 0; e < kSideInline; ++e) {
             pw[e] = 1.0;
             dm[e] = 1.0;
             if (e < n) {
-                const double x = w[c_off + ldg(M.sidx + b + e)];
-                const int ie = ldg(M.siexp + b + e);
-                const double se = ldg(M.sexp + b + e);
-                pw[e] = specie_pow(x, ie, se);
-                dm[e] = se * specie_pow_m1(x, ie, se);
+                const double x = w[c_off + R.idx[side][e]];
+                pw[e] = specie_pow(x, R.iexp[side][e], R.sexp[side][e]);
+                dm[e] = R.sexp[side][e] * specie_pow_m1(x, R.iexp[side][e], R.sexp[side][e]);
             }
         }
         double C = 1.0;
 #pragma unroll
-        for (int e = 0; e < kInlineSide; ++e)
+        for (int e = 0; e < kSideInline; ++e)
             if (e < n) C *= pw[e];
 #pragma unroll
-        for (int j = 0; j < kInlineSide; ++j) {
+        for (int j = 0; j < kSideInline; ++j) {
             if (j < n) {
                 double d = 1;
 #pragma unroll
-                for (int i = 0; i < kInlineSide; ++i)
+                for (int i = 0; i < kSideInline; ++i)
                     if (i < n) d *= (i == j) ? dm[i] : pw[i];
                 w[out + j] = d * kmul;
             }
         }
         return C;
     }
+    const int b = R.sp_off + (side ? R.nl : 0);
     double C = 1.0;
     for (int e = 0; e < n; ++e)
         C *= specie_pow(w[c_off + ldg(M.sidx + b + e)], ldg(M.siexp + b + e), ldg(M.sexp + b + e));
@@ -684,10 +750,11 @@ template <int G, class W>
 __device__ __forceinline__ void stage_jacobian_params(const Grp<G>& g, const DevMech& M, const W& w,
                                                       const WsLayout& L, const TCache& tc, bool use_cache) {
     for (int q = g.lane; q < M.nR; q += G) {
-        const int type = ldg(M.rtype + q);
-        const int sp = ldg(M.sp_off + q);
-        const int nl = ldg(M.nl + q), nr = ldg(M.nr + q);
-        const int so = ldg(M.slot + q);
+        Rxn R;
+        load_rxn(M, q, R);
+        const int type = R.type;
+        const int nl = R.nl;
+        const int so = R.slot;
         double ddT = 0.0, Ak = 0.0, kf;
         double cachedInvKc = 0.0;
         if (use_cache) {
@@ -696,36 +763,35 @@ __device__ __forceinline__ void stage_jacobian_params(const Grp<G>& g, const Dev
             kf = w[L.stage + so + 1];
             cachedInvKc = w[L.stage + so + 2];
             Ak = w[L.stage + so + 3];
-            const int f = (type == GF_RATE_LINDEMANN_FALLOFF || type == GF_RATE_TROE_FALLOFF) ? 1 : 0;
-            ddT = kf * arr_dlnkdT(M, q, f, tc);
+            const bool falloff = type == GF_RATE_LINDEMANN_FALLOFF || type == GF_RATE_TROE_FALLOFF;
+            ddT = kf * (falloff ? arr_dlnkdT1(M, q, tc) : arr_dlnkdT0(R, tc));
         } else {
-            const int tbr = ldg(M.tb_row + q);
-            kf = rate_k(M, q, type, tc, tbr >= 0 ? w[L.Mtb + tbr] : 0.0, true, &ddT, &Ak);
+            kf = rate_k(M, q, R, tc, R.tb_row >= 0 ? w[L.Mtb + R.tb_row] : 0.0, true, &ddT, &Ak);
         }
-        const double Cf = side_products(M, w, L.c, sp, nl, kf, L.stage + so + 2);
+        const double Cf = side_products(M, w, L.c, R, 0, kf, L.stage + so + 2);
         double dwdT = Cf * ddT;
         double omega = Cf * kf;
         double Cr = 0.0, invKc = 1.0;
-        if (!ldg(M.rirr + q)) {
+        if (!R.irr) {
             double Gstd;
             Poly7 a;
             if (use_cache) {
-                a = reaction_coeffs(M, q, tc.T);
+                a = reaction_coeffs_at(M, q, tc.T, R.Tcommon);
                 Gstd = th_Gstd(a, tc.T, tc.logT);
                 invKc = cachedInvKc;
             } else {
-                invKc = exp(-reaction_lnKc(M, q, tc, &Gstd, &a));
+                invKc = exp(-reaction_lnKc(M, q, R, tc, &Gstd, &a));
             }
-            const double dKcdTbyKc = reaction_dKcdTbyKc(M, q, tc, Gstd, a);
+            const double dKcdTbyKc = reaction_dKcdTbyKc(R, tc, Gstd, a);
             const double kr = kf * invKc;
-            Cr = side_products(M, w, L.c, sp + nl, nr, kr, L.stage + so + 2 + nl);
+            Cr = side_products(M, w, L.c, R, 1, kr, L.stage + so + 2 + nl);
             const double dkrdT = ddT * invKc - kr * dKcdTbyKc;
             dwdT -= Cr * dkrdT;
             omega -= Cr * kr;
         }
         w[L.stage + so] = omega;
         w[L.stage + so + 1] = dwdT;
-        if (type == GF_RATE_THIRD_BODY_ARRHENIUS) w[L.stage + so + 2 + nl + nr] = Ak * (Cf - Cr * invKc);
+        if (type == GF_RATE_THIRD_BODY_ARRHENIUS) w[L.stage + so + 2 + nl + R.nr] = Ak * (Cf - Cr * invKc);
     }
     g.sync();
 }
@@ -953,14 +1019,20 @@ __device__ __forceinline__ void lu_panel(const Grp<G>& g, const W& w, int A, int
 }
 
 // Panel steps k0 .. k1-1 with the panel held in registers (one full warp):
-// lane l holds panel rows k0 + l + 32 r (r < RP) and their row scalings.
-// Pivot search, the exchange of two panel rows, the column scaling and the
-// panel update run on registers and shuffles; the exchanges of the columns
-// outside the panel are left to lu_apply_swaps. Same operations, in the same
-// order per entry, as lu_panel. The pivots are stored to piv[]; the panel and
-// the updated row scalings are written back to A and vv.
-// Difference: when every candidate of a column is NaN, the reference exchanges
-// row k with row 0 (its iMax starts at 0); here no exchange is made (iMax = k).
+// register slot (lane l, r) holds a panel row (initially row k0 + l + 32 r)
+// with its row scaling, and a label: the row position it has in the
+// reference's matrix after the exchanges so far. An exchange of rows k and
+// iMax swaps the two slots' labels instead of moving data; the pivot search,
+// its tie-break ("last max wins" by position), the update condition and the
+// write-back all go by label. The row scaling stays with its data, which is
+// the reference's vv[iMax] = vv[k] (ludecompose.H:71-78); the scaling left at
+// position k is never read again. The pivot search reduces across lanes with
+// three integer warp reductions on order-preserving keys of the non-negative
+// candidates (high word, low word, then the largest position). Same
+// operations, in the same order per entry, as lu_panel. The pivots go to
+// piv[]; the exchanges of the columns outside the panel are left to
+// lu_apply_swaps. Difference: when every candidate of a column is NaN, the
+// reference exchanges row k with row 0 (its iMax starts at 0); here none is.
 template <int RP, int NB, class W>
 __device__ __forceinline__ void lu_panel_reg(const Grp<32>& g, const W& w, int A, int ld, int piv, int vv, int m,
                                              int k0, int k1) {
@@ -968,9 +1040,11 @@ __device__ __forceinline__ void lu_panel_reg(const Grp<32>& g, const W& w, int A
     const int kb = k1 - k0;
     double a[RP][NB];
     double sv[RP];
+    int lab[RP];
 #pragma unroll
     for (int r = 0; r < RP; ++r) {
         const int p = k0 + l + 32 * r;
+        lab[r] = p < m ? p : m;  // slots past the last row never qualify
 #pragma unroll
         for (int t = 0; t < NB; ++t) a[r][t] = (p < m && t < kb) ? w[A + p * ld + k0 + t] : 0.0;
         sv[r] = p < m ? w[vv + p] : 0.0;
@@ -979,82 +1053,67 @@ __device__ __forceinline__ void lu_panel_reg(const Grp<32>& g, const W& w, int A
     for (int kk = 0; kk < NB; ++kk) {
         if (kk >= kb) break;
         const int k = k0 + kk;
-        // pivot search: the last row with the largest vv * |a| (ludecompose.H:57-63)
+        // pivot search: the last position with the largest vv * |a| (ludecompose.H:57-63)
         double best = -1.0;
         int bi = -1;
 #pragma unroll
         for (int r = 0; r < RP; ++r) {
-            const int p = k0 + l + 32 * r;
-            if (p >= k && p < m) {
+            if (lab[r] >= k && lab[r] < m) {
                 const double t = sv[r] * fabs(a[r][kk]);
-                if (t >= best) {
+                if (t > best || (t == best && lab[r] > bi)) {
                     best = t;
-                    bi = p;
+                    bi = lab[r];
                 }
             }
         }
+        const bool has = bi >= 0;
+        const unsigned hi = has ? (unsigned)__double2hiint(best) : 0u;
+        const unsigned lo = has ? (unsigned)__double2loint(best) : 0u;
+        const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+        const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+        const int mr =
+            (int)__reduce_max_sync(0xffffffffu, (has && hi == mh && lo == ml) ? (unsigned)(bi + 1) : 0u) - 1;
+        const int iMax = mr < 0 ? k : mr;
+        // the slot that holds position iMax becomes position k, and the slot
+        // that held position k becomes iMax
+        int ri = -1;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi > bi)) {
-                best = ob;
-                bi = oi;
-            }
-        }
-        const int iMax = bi < 0 ? k : bi;
-        const int lk = (k - k0) & 31, rk = (k - k0) >> 5;
+        for (int r = 0; r < RP; ++r)
+            if (lab[r] == iMax) ri = r;
+        const unsigned own = __ballot_sync(0xffffffffu, ri >= 0);
+        const int li = __ffs(own) - 1;
+        ri = __shfl_sync(0xffffffffu, ri, li);
         if (iMax != k) {
-            // exchange panel rows k and iMax; vv[iMax] = vv[k] (:71-78)
-            const int li = (iMax - k0) & 31, ri = (iMax - k0) >> 5;
 #pragma unroll
-            for (int t = 0; t < NB; ++t) {
-                double xk = a[0][t], xi = a[0][t];
-#pragma unroll
-                for (int r = 1; r < RP; ++r) {
-                    if (r == rk) xk = a[r][t];
-                    if (r == ri) xi = a[r][t];
-                }
-                const double vk = __shfl_sync(0xffffffffu, xk, lk);
-                const double vi = __shfl_sync(0xffffffffu, xi, li);
-#pragma unroll
-                for (int r = 0; r < RP; ++r) {
-                    if (l == lk && r == rk) a[r][t] = vi;
-                    if (l == li && r == ri) a[r][t] = vk;
-                }
+            for (int r = 0; r < RP; ++r) {
+                if (lab[r] == k)
+                    lab[r] = iMax;
+                else if (lab[r] == iMax)
+                    lab[r] = k;
             }
-            double sk = sv[0];
-#pragma unroll
-            for (int r = 1; r < RP; ++r)
-                if (r == rk) sk = sv[r];
-            sk = __shfl_sync(0xffffffffu, sk, lk);
-#pragma unroll
-            for (int r = 0; r < RP; ++r)
-                if (l == li && r == ri) sv[r] = sk;
         }
         if (l == 0) w.ip(piv + k) = iMax;
-        // pivot row k of the panel, broadcast; a zero pivot becomes gpuSmall (:81)
+        // pivot row (now position k), broadcast; a zero pivot becomes gpuSmall (:81)
         double urow[NB];
 #pragma unroll
         for (int t = 0; t < NB; ++t) {
             double x = a[0][t];
 #pragma unroll
             for (int r = 1; r < RP; ++r)
-                if (r == rk) x = a[r][t];
-            urow[t] = (t >= kk && t < kb) ? __shfl_sync(0xffffffffu, x, lk) : 0.0;
+                if (r == ri) x = a[r][t];
+            urow[t] = (t >= kk && t < kb) ? __shfl_sync(0xffffffffu, x, li) : 0.0;
         }
         if (urow[kk] == 0.0) {
             urow[kk] = kSmall;
 #pragma unroll
             for (int r = 0; r < RP; ++r)
-                if (l == lk && r == rk) a[r][kk] = kSmall;
+                if (l == li && r == ri) a[r][kk] = kSmall;
         }
         if (k != m - 1) {
             const double rDiag = 1.0 / urow[kk];
 #pragma unroll
             for (int r = 0; r < RP; ++r) {
-                const int p = k0 + l + 32 * r;
-                if (p > k && p < m) {
+                if (lab[r] > k && lab[r] < m) {
                     const double lik = a[r][kk] * rDiag;
                     a[r][kk] = lik;
 #pragma unroll
@@ -1066,12 +1125,11 @@ __device__ __forceinline__ void lu_panel_reg(const Grp<32>& g, const W& w, int A
     }
 #pragma unroll
     for (int r = 0; r < RP; ++r) {
-        const int p = k0 + l + 32 * r;
-        if (p < m) {
+        if (lab[r] < m) {
 #pragma unroll
             for (int t = 0; t < NB; ++t)
-                if (t < kb) w[A + p * ld + k0 + t] = a[r][t];
-            w[vv + p] = sv[r];
+                if (t < kb) w[A + lab[r] * ld + k0 + t] = a[r][t];
+            w[vv + lab[r]] = sv[r];
         }
     }
 }

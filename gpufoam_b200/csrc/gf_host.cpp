@@ -418,6 +418,33 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
                 for (int c = 0; c < nS; ++c) add(x.rhs[i].index, c, sp, x.rhs[i].stoich * x.efficiencies[c]);
         }
     }
+    std::vector<RxnHead> rxh(nRa);
+    std::vector<RxnSpecie> rxs((size_t)nRa * 2 * kSideInline, RxnSpecie{0, 1, 1.0});
+    for (int q = 0; q < nR; ++q) {
+        RxnHead& h = rxh[q];
+        h.type = rtype[q];
+        h.irr = rirr[q];
+        h.slot = slot[q];
+        h.tb_row = tb_row[q];
+        h.nl = nl[q];
+        h.nr = nr[q];
+        h.sp_off = sp_off[q];
+        h.nm_small = rnm_small[q];
+        h.lnA0 = lnA0[q];
+        h.beta0 = beta0[q];
+        h.Ta0 = Ta0[q];
+        h.sA0 = sA0[q];
+        h.Tcommon = rTc[q];
+        h.Y = rY[q];
+        h.nm = rnm[q];
+        h.pad = 0.0;
+        for (int side = 0; side < 2; ++side) {
+            const int n = side == 0 ? nl[q] : nr[q];
+            const int b = sp_off[q] + (side == 0 ? 0 : nl[q]);
+            for (int e = 0; e < n && e < kSideInline; ++e)
+                rxs[((size_t)q * 2 + side) * kSideInline + e] = RxnSpecie{sidx[b + e], siexp[b + e], sexp[b + e]};
+        }
+    }
     const int ldJ = (nS + 1) | 1;  // the workspace Jacobian row stride (make_layout)
     std::vector<int> dn_pos(nS), je_pos(nE);
     for (int s2 = 0; s2 < nS; ++s2) dn_pos[s2] = s2;
@@ -445,7 +472,7 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
                  oRc = b.add(rcoef), oLA0 = b.add(lnA0), oSA0 = b.add(sA0), oB0 = b.add(beta0), oT0 = b.add(Ta0),
                  oLA1 = b.add(lnA1), oSA1 = b.add(sA1), oB1 = b.add(beta1), oT1 = b.add(Ta1), oTroe = b.add(troe),
                  oTb = b.add(tb_row), oEff = b.add(eff), oSi = b.add(sidx), oSie = b.add(siexp), oSst = b.add(sst),
-                 oSe = b.add(sexp);
+                 oSe = b.add(sexp), oRxh = b.add(rxh), oRxs = b.add(rxs);
     size_t oDst[kNumGroupSizes], oJst[kNumGroupSizes];
     for (int k = 0; k < kNumGroupSizes; ++k) {
         oDst[k] = b.add(dst_rec[k]);
@@ -502,6 +529,8 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     D.troe = (const double*)P(oTroe);
     D.tb_row = (const int*)P(oTb);
     D.eff = (const double*)P(oEff);
+    D.rxh = (const RxnHead*)P(oRxh);
+    D.rxs = (const RxnSpecie*)P(oRxs);
     D.sidx = (const int*)P(oSi);
     D.siexp = (const int*)P(oSie);
     D.sst = (const double*)P(oSst);

@@ -12,6 +12,22 @@ namespace gf {
 constexpr int kMaxW = GF_MAX_REACTION_WIDTH;
 constexpr int kNoIntExp = 2147483647 / 10;  // gpuLabelMax: "not an integer exponent"
 
+// Packed per-reaction data (compute order q), loaded with a handful of
+// independent 16-byte loads: the head and up to kSideInline species per side.
+struct __align__(16) RxnHead {
+    int type, irr, slot, tb_row;   // tb_row: row of eff, -1 for plain Arrhenius
+    int nl, nr, sp_off, nm_small;  // nm_small: Kc = K (gpuThermo.H:111)
+    double lnA0, beta0, Ta0, sA0;  // k (or the fall-off k0): ln|A|, beta, Ta, sign(A)
+    double Tcommon, Y, nm, pad;    // the reaction ΔThermo's Tcommon, Y and Y / W
+};
+constexpr int kSideInline = 4;
+// species entry of a reaction side: index, integer exponent (or kNoIntExp), exponent
+struct __align__(16) RxnSpecie {
+    int idx;
+    int iexp;
+    double exp;
+};
+
 // One record of a gather stream: acc += coef * src[slot] (slot < 0: nothing);
 // pos >= 0 marks the last record of an output entry: dst[pos] = acc, acc = 0.
 struct __align__(16) StreamRec {
@@ -88,6 +104,8 @@ struct DevMech {
     const double* troe;        // [nR][4]: alpha, 1/Tsss, 1/Ts, Tss
     const int* tb_row;         // [nR] row of eff, -1 for plain Arrhenius
     const double* eff;         // [n_tb][nS]
+    const RxnHead* rxh;        // [nR]
+    const RxnSpecie* rxs;      // [nR][2 * kSideInline]: lhs, then rhs (wider sides: sidx/siexp/sexp)
     const int* sidx;
     const int* siexp;          // integer exponent or kNoIntExp
     const double* sst;
