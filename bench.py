@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint measurement (4096 GRI-size cells, deltaT 1e-4 s)")
     return ap.parse_args()
 
 
@@ -200,6 +202,56 @@ def cpu_reference_rate(batch, solver, dT, seconds, nthreads, offset=0):
         done_all += done
         t_all += t
     return n / t_inv, done_all, kind, t_all
+
+
+ADJOINT = dict(mech="gri", n=4096, dT=1e-4, T=(1100.0, 1600.0))
+
+
+def adjoint_measure(solver_launch, steps):
+    """Forward (plain solve and recording solve) and adjoint sweep times on the
+    differentiation workload: 4096 GRI-size cells, T ~ U[1100, 1600] K, deltaT
+    1e-4 s (through ignition), Rosenbrock34; loss = seeded weights . final (Y, T).
+    Gradients w.r.t. the initial states and all (ln|A|, beta, Ta) per reaction."""
+    import torch
+    from gpufoam_b200 import adjoint as AD
+    from gpufoam_b200 import evaluator as E
+    from gpufoam_b200 import mechanism as M
+    raw = M.gri_size(0)
+    cells = M.make_cells(raw, ADJOINT["n"], seed=4096, T_range=ADJOINT["T"])
+    ode = E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4)
+    sol = AD.AdjointSolver(raw, ode, traj_cap=4096, launch=solver_launch)
+    Y0 = torch.as_tensor(cells, device="cuda")
+    w = torch.as_tensor(np.random.default_rng(5).standard_normal(cells.shape), device="cuda")
+    w[:, raw.n_species + 1] = 0.0
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    fw, rec, adj = [], [], []
+    for k in range(steps + 1):
+        dtc = torch.full((ADJOINT["n"],), DTC0, dtype=torch.float64, device="cuda")
+        a0, a1 = ev()
+        a0.record()
+        sol.solver.solve(Y0, ADJOINT["dT"], dtc, want_status=False, want_counters=False, want_stats=False)
+        a1.record()
+        dtc = torch.full((ADJOINT["n"],), DTC0, dtype=torch.float64, device="cuda")
+        b0, b1 = ev()
+        b0.record()
+        Y1, status, counters = sol.forward(Y0, ADJOINT["dT"], dtc)
+        b1.record()
+        c0, c1 = ev()
+        c0.record()
+        Y0bar, thb, st = sol.backward(w)
+        c1.record()
+        torch.cuda.synchronize()
+        if k > 0:
+            fw.append(a0.elapsed_time(a1))
+            rec.append(b0.elapsed_time(b1))
+            adj.append(c0.elapsed_time(c1))
+    cnt = counters.cpu().numpy()
+    ok = int(((status.cpu().numpy() == 0) & (st.cpu().numpy() == 0)).sum())
+    f, r, a = float(np.mean(fw)), float(np.mean(rec)), float(np.mean(adj))
+    return {"workload": "4096 GRI-size cells, T~U[1100,1600] K, deltaT 1e-4 s, Rosenbrock34",
+            "forward_ms": f, "forward_recording_ms": r, "adjoint_ms": a, "adjoint_over_forward": a / f,
+            "accepted_steps_per_cell": {"mean": float(cnt[:, 0].mean()), "max": int(cnt[:, 0].max())},
+            "cells_ok": ok, "parameters": f"{raw.n_reactions} x (ln|A|, beta, Ta)"}
 
 
 def main():
@@ -409,6 +461,10 @@ def main():
                "d2h_bytes_per_step": int(n * (cells.shape[1] + 1) * 8),
                "api": "Solver.solve -> gf_solve with per-cell deltaT and mechanism id (pinned host arrays)"}
 
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint and batch.mech_id is None:
+        adjoint = adjoint_measure(solver.get_launch(), 1)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         r, done, kind, t = cpu_reference_rate(batch, args.solver, wl["dT"], args.cpu_seconds, nthreads)
@@ -433,6 +489,7 @@ def main():
             "plain": plain,
             "persistent_vs_plain": (value / plain["value"]) if plain else None,
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
+            "adjoint": adjoint,
         }
         print(json.dumps(line))
     if world > 1:

@@ -29,6 +29,7 @@ EXPORTS = [
     "gf_solver_create", "gf_solver_destroy", "gf_solver_set_launch", "gf_solver_get_launch", "gf_solve",
     "gf_compute_rr", "gf_compute_ynew", "gf_rates", "gf_jacobian", "gf_lu_decompose", "gf_lu_backsubstitute",
     "gf_strerror", "gf_abi_version", "gf_last_cuda_error", "gf_measure_fp64_peak", "gf_solve_noalloc",
+    "gf_solve_record", "gf_adjoint",
 ]
 
 
@@ -126,6 +127,8 @@ def load() -> C.CDLL:
     lib.gf_measure_fp64_peak.argtypes = [dp, P(dp)]
     lib.gf_solve_noalloc.argtypes = [vp, P(GfOdeInputs), dp, ip, dp, vp, dp, vp, vp, ip, vp, vp, vp, ip, vp, vp,
                                      P(GfStats), vp]
+    lib.gf_solve_record.argtypes = [vp, ip, dp, vp, ip, vp, vp, vp, vp, vp, ip, vp]
+    lib.gf_adjoint.argtypes = [vp, ip, vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, vp, vp]
     lib.gf_strerror.argtypes = [ip]
     lib.gf_strerror.restype = C.c_char_p
     lib.gf_abi_version.restype = ip

@@ -1559,7 +1559,8 @@ __device__ __forceinline__ double ros_d(const RosCoeffs& C, int i) {
 // candidate is written to yt_off.
 template <int G, class W>
 __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
-                              const OdeParams& o, int y0_off, int yt_off, double p, double dx) {
+                              const OdeParams& o, int y0_off, int yt_off, double p, double dx, int save_y2 = -1,
+                              int save_y3 = -1) {
     const int m = M.m;
     const int ld = L.ld;
     jacobian(g, M, w, L, y0_off, p, true);
@@ -1593,12 +1594,14 @@ __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M,
     for (int st = 0; st < C.s; ++st) {
         const int ki = L.k1 + st * m;
         if (st == 1 || (st == 2 && C.s == 4)) {
+            // the stage point (kept at save_y2 / save_y3 when asked: the adjoint sweep)
+            const int pt = (st == 1 && save_y2 >= 0) ? save_y2 : ((st == 2 && save_y3 >= 0) ? save_y3 : yt_off);
             for (int i = g.lane; i < m; i += G) {
                 double v = w[y0_off + i];
                 for (int j = 0; j < st; ++j) v += ros_a(C, st, j) * w[L.k1 + j * m + i];
-                w[yt_off + i] = v;
+                w[pt + i] = v;
             }
-            derivatives(g, M, w, L, yt_off, p, L.dydx);
+            derivatives(g, M, w, L, pt, p, L.dydx);
         }
         const int src = st == 0 ? L.dydx0 : L.dydx;
         const double dd = dx * ros_d(C, st);
@@ -1652,7 +1655,8 @@ struct CellResult {
 template <int G, class W>
 __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const OdeParams& o,
                          const RosCoeffs& C, double xStart, double xEnd, int* y_off, int* yt_off, double p,
-                         double* dxTry, int* accepted, int* attempts) {
+                         double* dxTry, int* accepted, int* attempts, double* rec = nullptr, int rec_cap = 0,
+                         int rec_ld = 0) {
     double step_dxTry = *dxTry;
     bool last = false;
     double x = xStart;
@@ -1681,6 +1685,13 @@ __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, cons
             }
         } while (err > 1.0);
         x += dx;
+        if (rec) {
+            // the accepted step's start state and size, for the adjoint sweep
+            if (*accepted >= rec_cap) return GF_CELL_MAX_STEPS;
+            double* r = rec + (size_t)(*accepted) * rec_ld;
+            for (int i = g.lane; i < M.m; i += G) r[i] = w[*y_off + i];
+            if (g.lane == 0) r[M.m] = dx;
+        }
         const int t = *y_off;
         *y_off = *yt_off;
         *yt_off = t;
@@ -1727,7 +1738,9 @@ __device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, 
         double timeLeft = dT;
         while (timeLeft > kSmall) {
             const double dt = timeLeft;
-            const int st = ode_solve(g, M, w, L, a.ode, C, 0.0, dt, &y_off, &yt_off, p, &dxTry, &accepted, &attempts);
+            double* rec = a.traj ? a.traj + (size_t)cell * a.traj_cap * a.traj_ld : nullptr;
+            const int st = ode_solve(g, M, w, L, a.ode, C, 0.0, dt, &y_off, &yt_off, p, &dxTry, &accepted, &attempts,
+                                     rec, a.traj_cap, a.traj_ld);
             if (st != GF_CELL_OK && status == GF_CELL_OK) status = st;
             if (st == GF_CELL_STEP_UNDERFLOW) break;
             int bad = 0;

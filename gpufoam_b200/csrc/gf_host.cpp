@@ -162,6 +162,8 @@ struct gf_solver {
     unsigned long long* queue_host = nullptr;  // pinned
     double* ws = nullptr;
     size_t ws_bytes = 0;
+    double* adj_ws = nullptr;  // the adjoint sweep's workspaces
+    size_t adj_ws_bytes = 0;
     int max_ws_doubles = 0;
     int max_neq = 0;
     // device staging for the host-memory entry points
@@ -449,11 +451,24 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     std::vector<int> dn_pos(nS), je_pos(nE);
     for (int s2 = 0; s2 < nS; ++s2) dn_pos[s2] = s2;
     for (int e = 0; e < nE; ++e) je_pos[e] = (e / (nS + 1)) * ldJ + e % (nS + 1);
-    std::vector<std::vector<StreamRec>> dst_rec(kNumGroupSizes), jst_rec(kNumGroupSizes);
-    int dst_len[kNumGroupSizes], jst_len[kNumGroupSizes];
+    // concentration gathers of the adjoint: species s <- entry slots of its occurrences
+    std::vector<std::vector<std::pair<int, double>>> cg(nS);
+    int max_side = 0;
+    for (int q = 0; q < nR; ++q) {
+        max_side = std::max(max_side, std::max(nl[q], nr[q]));
+        for (int side = 0; side < 2; ++side) {
+            const int n = side == 0 ? nl[q] : nr[q];
+            const int b = sp_off[q] + (side == 0 ? 0 : nl[q]);
+            for (int e = 0; e < n && e < kSideInline; ++e)
+                cg[sidx[b + e]].push_back({q * 2 * kSideInline + side * kSideInline + e, 1.0});
+        }
+    }
+    std::vector<std::vector<StreamRec>> dst_rec(kNumGroupSizes), jst_rec(kNumGroupSizes), cst_rec(kNumGroupSizes);
+    int dst_len[kNumGroupSizes], jst_len[kNumGroupSizes], cst_len[kNumGroupSizes];
     for (int k = 0; k < kNumGroupSizes; ++k) {
         dst_rec[k] = build_stream(dn, dn_pos, 1 << k, &dst_len[k]);
         jst_rec[k] = build_stream(je, je_pos, 1 << k, &jst_len[k]);
+        cst_rec[k] = build_stream(cg, dn_pos, 1 << k, &cst_len[k]);
     }
     // keep every array non-empty
     if (eff.empty()) eff.push_back(0.0);
@@ -472,11 +487,12 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
                  oRc = b.add(rcoef), oLA0 = b.add(lnA0), oSA0 = b.add(sA0), oB0 = b.add(beta0), oT0 = b.add(Ta0),
                  oLA1 = b.add(lnA1), oSA1 = b.add(sA1), oB1 = b.add(beta1), oT1 = b.add(Ta1), oTroe = b.add(troe),
                  oTb = b.add(tb_row), oEff = b.add(eff), oSi = b.add(sidx), oSie = b.add(siexp), oSst = b.add(sst),
-                 oSe = b.add(sexp), oRxh = b.add(rxh), oRxs = b.add(rxs);
-    size_t oDst[kNumGroupSizes], oJst[kNumGroupSizes];
+                 oSe = b.add(sexp), oRxh = b.add(rxh), oRxs = b.add(rxs), oRofq = b.add(qof);
+    size_t oDst[kNumGroupSizes], oJst[kNumGroupSizes], oCst[kNumGroupSizes];
     for (int k = 0; k < kNumGroupSizes; ++k) {
         oDst[k] = b.add(dst_rec[k]);
         oJst[k] = b.add(jst_rec[k]);
+        oCst[k] = b.add(cst_rec[k]);
     }
     gf_mech* m = new (std::nothrow) gf_mech;
     if (!m) return GF_ERR_OUT_OF_MEMORY;
@@ -529,6 +545,7 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     D.troe = (const double*)P(oTroe);
     D.tb_row = (const int*)P(oTb);
     D.eff = (const double*)P(oEff);
+    D.r_of_q = (const int*)P(oRofq);
     D.rxh = (const RxnHead*)P(oRxh);
     D.rxs = (const RxnSpecie*)P(oRxs);
     D.sidx = (const int*)P(oSi);
@@ -538,7 +555,9 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     for (int k = 0; k < kNumGroupSizes; ++k) {
         D.dst[k] = Stream{(const StreamRec*)P(oDst[k]), dst_len[k]};
         D.jst[k] = Stream{(const StreamRec*)P(oJst[k]), jst_len[k]};
+        D.cst[k] = Stream{(const StreamRec*)P(oCst[k]), cst_len[k]};
     }
+    D.max_side = max_side;
     *out = m;
     return GF_OK;
 }
@@ -598,6 +617,7 @@ void gf_solver_destroy(gf_solver* s) {
     cudaFree(s->queue);
     if (s->queue_host) cudaFreeHost(s->queue_host);
     cudaFree(s->ws);
+    cudaFree(s->adj_ws);
     cudaFree(s->dY);
     cudaFree(s->dYnew);
     cudaFree(s->dRR);
@@ -687,6 +707,82 @@ int gf_solve(gf_solver* s, int n_cells, double deltaT, const double* deltaT_cell
         stats->failed_cells = (long long)s->queue_host[4];
     }
     return GF_OK;
+}
+
+// gf_solve with the trajectory recorded for the adjoint (single mechanism).
+int gf_solve_record(gf_solver* s, int n_cells, double deltaT, const double* Y0, int ld_y, double* Ynew,
+                    double* deltaTChem, int* status, int* counters, double* traj, int traj_cap, void* stream) {
+    if (!s || n_cells < 0 || !Y0 || !Ynew || !deltaTChem || !status || !counters || !traj || traj_cap < 1)
+        return GF_ERR_INVALID_ARGUMENT;
+    if (s->mechs.size() != 1 || ld_y < s->max_neq) return GF_ERR_INVALID_ARGUMENT;
+    gf::LaunchArgs a;
+    a.n_cells = n_cells;
+    a.deltaT = deltaT;
+    a.deltaT_cell = nullptr;
+    a.deltaTChemMax = INFINITY;
+    a.mech_id = nullptr;
+    a.rho = nullptr;
+    a.Y0 = Y0;
+    a.ld_y = ld_y;
+    a.Ynew = Ynew;
+    a.deltaTChem = deltaTChem;
+    a.RR = nullptr;
+    a.ld_rr = 0;
+    a.status = status;
+    a.counters = counters;
+    a.Treact = s->Treact;
+    a.ode = s->ode;
+    a.queue = s->queue;
+    a.traj = traj;
+    a.traj_cap = traj_cap;
+    a.traj_ld = s->dmechs[0].m + 1;
+    const int wsd = s->max_ws_doubles;
+    int slots = 0;
+    a.ws_slot_stride = 0;
+    if (s->cfg.kind == 0) {
+        slots = n_cells;
+        a.ws_slot_stride = n_cells;
+    } else {
+        int blocks = 0, threads = 0;
+        slots = gf::persistent_slots(s->cfg, wsd * (int)sizeof(double), &blocks, &threads);
+        if (slots <= 0) return GF_ERR_UNSUPPORTED;
+        if (s->cfg.scratch_in_shared) slots = 0;
+    }
+    if (slots > 0) {
+        const int r = ensure_ws(s, (size_t)slots * wsd * sizeof(double));
+        if (r) return r;
+    }
+    a.ws = s->ws;
+    const int ce = gf::launch_cells(s->dmechs.data(), 1, s->cfg, a, wsd, slots, stream);
+    return ce ? cuda_fail((cudaError_t)ce) : GF_OK;
+}
+
+// The reverse sweep over a recorded trajectory (gf_adjoint.cu).
+int gf_adjoint(gf_solver* s, int n_cells, const double* traj, int traj_cap, const int* counters,
+               const int* fwd_status, const double* Y0, const double* Ynew, const double* Ybar, int ld_y,
+               double* Y0bar, double* theta_bar, int* status, void* stream) {
+    if (!s || n_cells < 0 || !traj || traj_cap < 1 || !counters || !fwd_status || !Y0 || !Ynew || !Ybar ||
+        !Y0bar || !theta_bar || !status)
+        return GF_ERR_INVALID_ARGUMENT;
+    if (s->mechs.size() != 1 || ld_y < s->max_neq) return GF_ERR_INVALID_ARGUMENT;
+    const gf::DevMech& M = s->dmechs[0];
+    if (M.max_side > gf::kSideInline) return GF_ERR_UNSUPPORTED;
+    const int per_sm = gf::adjoint_blocks_per_sm();
+    if (per_sm < 1) return GF_ERR_CUDA;
+    const int blocks = per_sm * gf::device_sm_count();
+    const long long wsd = gf::adjoint_ws_doubles(M);
+    const size_t bytes = (size_t)blocks * wsd * sizeof(double);
+    if (bytes > s->adj_ws_bytes) {
+        cudaFree(s->adj_ws);
+        s->adj_ws = nullptr;
+        s->adj_ws_bytes = 0;
+        GF_CUDA(cudaMalloc(&s->adj_ws, bytes));
+        s->adj_ws_bytes = bytes;
+    }
+    const int e = gf::launch_adjoint_cells(M, n_cells, traj, traj_cap, counters, fwd_status, Y0, Ynew, Ybar, ld_y,
+                                           Y0bar, theta_bar, status, s->ode, s->adj_ws, wsd, blocks, s->queue,
+                                           stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
 }
 
 static int host_solve(gf_solver* s, int n, double deltaT, double deltaTChemMax, const double* rho,

@@ -104,6 +104,7 @@ struct DevMech {
     const double* troe;        // [nR][4]: alpha, 1/Tsss, 1/Ts, Tss
     const int* tb_row;         // [nR] row of eff, -1 for plain Arrhenius
     const double* eff;         // [n_tb][nS]
+    const int* r_of_q;         // [nR] mechanism index of the reaction in compute position q
     const RxnHead* rxh;        // [nR]
     const RxnSpecie* rxs;      // [nR][2 * kSideInline]: lhs, then rhs (wider sides: sidx/siexp/sexp)
     const int* sidx;
@@ -112,6 +113,10 @@ struct DevMech {
     const double* sexp;
     Stream dst[kNumGroupSizes];
     Stream jst[kNumGroupSizes];
+    // the adjoint's concentration gathers: per species s, the per-reaction
+    // entry slots q * 2 * kSideInline + e whose species is s
+    Stream cst[kNumGroupSizes];
+    int max_side;              // most species on one side of a reaction
 };
 
 struct OdeParams {
@@ -151,6 +156,13 @@ struct LaunchArgs {
     double* ws;                    // workspaces
     long long ws_slot_stride;      // doubles per slot (blocked) or number of slots (interleaved)
     unsigned long long* queue;     // [0] next cell, [1] min deltaTChem bits, [2] accepted, [3] attempts, [4] failed
+    // optional trajectory record (the adjoint's forward pass): for accepted
+    // step k of a cell, traj[(cell * traj_cap + k) * traj_ld + 0 .. m) = the
+    // state at its start and [m] = its step size; a cell that takes more than
+    // traj_cap accepted steps records the first traj_cap and reports MAX_STEPS
+    double* traj = nullptr;
+    int traj_cap = 0;
+    int traj_ld = 0;
 };
 
 // Kernel launchers (gf_kernels.cu). All return a cudaError_t as int.
@@ -162,6 +174,15 @@ int launch_jacobian(const DevMech& m, int n, const double* y, double* dfdx, doub
 int launch_lu(int n_mats, int m, double* A, int* piv, double* vv, void* stream);
 int launch_lusolve(int n_mats, int m, const double* LU, const int* piv, double* b, void* stream);
 int launch_epilogue_reset(unsigned long long* queue, void* stream);
+
+// The discrete adjoint (gf_adjoint.cu).
+struct AdjArgs;
+int adjoint_ws_doubles(const DevMech& m);
+int launch_adjoint_cells(const DevMech& m, int n_cells, const double* traj, int traj_cap, const int* counters,
+                         const int* fwd_status, const double* Y0, const double* Ynew, const double* Ybar, int ld_y,
+                         double* Y0bar, double* theta_bar, int* status, const OdeParams& ode, double* ws,
+                         long long ws_per_cell, int n_blocks, unsigned long long* queue, void* stream);
+int adjoint_blocks_per_sm();
 
 // Device tables of a mechanism object (gf_host.cpp).
 const DevMech* mech_device_tables(const gf_mech* m);

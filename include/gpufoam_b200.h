@@ -224,6 +224,32 @@ int gf_compute_ynew(gf_solver* solver, int n_cells, double deltaT, double deltaT
                     const double* deltaTChem, const double* Y, double* Ynew,
                     double* deltaTChemNew);
 
+/* ---- differentiation (no counterpart in the reference) ------------------ */
+
+/* gf_solve (single mechanism, one flow step deltaT, no RR) that also records
+ * the trajectory for gf_adjoint: for accepted step k of cell c,
+ * traj[(c * traj_cap + k) * (nS + 2) + 0 .. nS] = the state (Y, T) at the step's
+ * start and [nS + 1] = its size. status and counters [n][2] (accepted,
+ * attempts) are required. A cell with more than traj_cap accepted steps stops
+ * with status GF_CELL_MAX_STEPS. Device pointers. */
+int gf_solve_record(gf_solver* solver, int n_cells, double deltaT, const double* Y0, int ld_y,
+                    double* Ynew, double* deltaTChem, int* status, int* counters,
+                    double* traj, int traj_cap, void* stream);
+
+/* Discrete adjoint of the recorded integration (step sequence frozen): given
+ * the loss gradient Ybar w.r.t. the final states Ynew, writes the gradient
+ * w.r.t. the initial states Y0 (Y and T; p gets 0) and, per cell,
+ * theta_bar[c][3 r + 0..2] = dL/d ln|A|, dL/d beta, dL/d Ta of reaction r
+ * (mechanism order; the k rate, k0 for fall-off reactions; Ta = Ea / R).
+ * traj, counters and fwd_status come from gf_solve_record with the same
+ * solver; status gets 0 per cell, or the recording's failure status (the
+ * cell's gradient is then 0). GF_ERR_UNSUPPORTED for reactions with more
+ * than 4 species on a side. Device pointers. */
+int gf_adjoint(gf_solver* solver, int n_cells, const double* traj, int traj_cap,
+               const int* counters, const int* fwd_status, const double* Y0, const double* Ynew,
+               const double* Ybar, int ld_y, double* Y0bar, double* theta_bar, int* status,
+               void* stream);
+
 /* Size of the static device scratch of gf_solve_noalloc (32 MiB per GPU). */
 #define GF_NOALLOC_SCRATCH_BYTES (32ll * 1024 * 1024)
 

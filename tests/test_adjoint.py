@@ -1,0 +1,142 @@
+"""Discrete adjoint (gf_solve_record / gf_adjoint) against the oracle.
+
+The oracle (oracle/gf_oracle.c, pinned to the reference) replays the recorded
+accepted steps with the step sequence frozen: y_{k+1} = Rosenbrock attempt(y_k,
+f(y_k), h_k), then the final max(0, Y) clip of singleCellSolver. Checks:
+
+* initial state: central differences with a relative step of 1e-6 of that map
+  along a random direction (all species, T, every cell), to 1e-5 relative;
+* per-reaction (ln|A|, beta, Ta) on random parameters: central differences with
+  relative steps 1e-4 and 2e-4, Richardson-extrapolated (a 1e-6 step is below
+  the loss's rounding noise for the small parameter gradients), to 1e-5
+  relative, or 1e-5 of the largest parameter gradient for the tiny ones;
+* a tangent-linear reference on the CPU: a tangent propagated through the
+  recorded steps by directional derivatives of each step map (central, relative
+  step 1e-7), against the adjoint's gradient along the same direction.
+"""
+import numpy as np
+import pytest
+
+from gpufoam_b200 import adjoint as AD
+from gpufoam_b200 import evaluator as E
+from gpufoam_b200 import mechanism as M
+from oracle.oracle import Oracle, ode_inputs
+
+
+def step_map(orc, inputs, y, h):
+    dydx = orc.derivatives(y[None])[0]
+    return orc.attempt(inputs, y[None], dydx[None], h)[0][0]
+
+
+def frozen_map(orc, inputs, y0, steps, nS):
+    y = np.array(y0, dtype=np.float64)
+    for h in steps:
+        y = step_map(orc, inputs, y, h)
+    y[:nS] = np.maximum(y[:nS], 0.0)
+    return y
+
+
+def test_parameters_roundtrip():
+    raw = M.h2_size(0)
+    th = AD.parameters_of(raw)
+    raw2 = AD.with_parameters(raw, th + 0.0)
+    for a, b in zip(raw.reactions, raw2.reactions):
+        assert a.A == pytest.approx(b.A, rel=1e-14) and a.beta == b.beta and a.Ta == b.Ta
+
+
+class Case:
+    """One recorded integration on the GPU, its adjoint, and the oracle's
+    frozen-step replay."""
+
+    def __init__(self, raw, n_cells, deltaT, solver, seed):
+        import torch
+        self.raw, self.nS, self.n = raw, raw.n_species, n_cells
+        self.cells = M.make_cells(raw, n_cells, seed=seed)
+        sol = AD.AdjointSolver(raw, E.OdeInputs(f"Rosenbrock{solver}", absTol=1e-8, relTol=1e-4), traj_cap=2048)
+        Y0 = torch.as_tensor(self.cells, device="cuda")
+        dtc = torch.full((n_cells,), 1e-7, dtype=torch.float64, device="cuda")
+        Y1, status, counters = sol.forward(Y0, deltaT, dtc)
+        torch.cuda.synchronize()
+        assert (status.cpu().numpy() == 0).all()
+        rng = np.random.default_rng(seed + 1)
+        self.rng = rng
+        self.w = rng.standard_normal((n_cells, self.nS + 2))
+        self.w[:, self.nS] *= 1e-3  # T in K against mass fractions
+        self.w[:, self.nS + 1] = 0.0
+        Y0bar, thb, st = sol.backward(torch.as_tensor(self.w, device="cuda"))
+        torch.cuda.synchronize()
+        assert (st.cpu().numpy() == 0).all()
+        self.Y0bar, self.thb = Y0bar.cpu().numpy(), thb.cpu().numpy()
+        traj = sol._rec["traj"].cpu().numpy()
+        cnt = counters.cpu().numpy()
+        self.steps = [traj[c, :cnt[c, 0], self.nS + 1] for c in range(n_cells)]
+        self.Y1 = Y1.cpu().numpy()
+        self.inp = ode_inputs(solver)
+        self.orc = Oracle(raw, "port")
+
+    def loss(self, orc, cells):
+        return sum(float(np.dot(self.w[c], frozen_map(orc, self.inp, cells[c], self.steps[c], self.nS)))
+                   for c in range(self.n))
+
+    def theta_loss(self, theta):
+        return self.loss(Oracle(AD.with_parameters(self.raw, theta), "port"), self.cells)
+
+
+def check_case(case, n_params):
+    nS, cells = case.nS, case.cells
+    # the replay reproduces the GPU integration
+    for c in range(case.n):
+        yf = frozen_map(case.orc, case.inp, cells[c], case.steps[c], nS)
+        np.testing.assert_allclose(yf, case.Y1[c], rtol=1e-10, atol=1e-14)
+    # initial state, random direction, central FD (relative step 1e-6)
+    d = case.rng.standard_normal(cells.shape)
+    d[:, nS + 1] = 0.0
+    scale = np.abs(cells) + 1e-6
+    eps = 1e-6
+    fd = (case.loss(case.orc, cells + eps * scale * d) - case.loss(case.orc, cells - eps * scale * d)) / (2 * eps)
+    ad = float(np.sum(case.Y0bar * scale * d))
+    assert abs(ad - fd) <= 1e-5 * abs(fd), ("initial state", ad, fd)
+    # tangent-linear reference along the same direction
+    tl = 0.0
+    for c in range(case.n):
+        y = np.array(cells[c])
+        t = scale[c] * d[c]
+        for h in case.steps[c]:
+            e = 1e-7 * np.linalg.norm(y[:nS + 1]) / max(np.linalg.norm(t[:nS + 1]), 1e-300)
+            t = (step_map(case.orc, case.inp, y + e * t, h) - step_map(case.orc, case.inp, y - e * t, h)) / (2 * e)
+            y = step_map(case.orc, case.inp, y, h)
+        t[:nS] = np.where(y[:nS] > 0.0, t[:nS], 0.0)
+        tl += float(np.dot(case.w[c], t))
+    assert abs(ad - tl) <= 1e-5 * abs(tl), ("tangent-linear", ad, tl)
+    # parameters: Richardson-extrapolated central differences
+    th0 = AD.parameters_of(case.raw)
+    picks = {(int(case.rng.integers(case.raw.n_reactions)), int(case.rng.integers(3))) for _ in range(n_params)}
+    gmax = np.abs(case.thb).max()
+    for r, k in sorted(picks):
+        def fd_at(hr):
+            step = hr * max(abs(th0[r, k]), 1.0)
+            tp, tm = th0.copy(), th0.copy()
+            tp[r, k] += step
+            tm[r, k] -= step
+            return (case.theta_loss(tp) - case.theta_loss(tm)) / (2 * step)
+        fd = (4.0 * fd_at(1e-4) - fd_at(2e-4)) / 3.0
+        ad = float(case.thb[r, k])
+        assert abs(ad - fd) <= 1e-5 * max(abs(fd), gmax), (r, k, ad, fd, gmax)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", [34, 23, 12])
+def test_adjoint_h2size(solver):
+    check_case(Case(M.h2_size(0), 3, 1e-5, solver, seed=11 + solver), n_params=64)
+
+
+@pytest.mark.gpu
+def test_adjoint_coverage_mechanism():
+    """Every rate type (Arrhenius, third body, Lindemann and Troe fall-off),
+    irreversible reactions and non-integer exponents."""
+    check_case(Case(M.coverage(0), 3, 1e-5, 34, seed=7), n_params=64)
+
+
+@pytest.mark.gpu
+def test_adjoint_grisize():
+    check_case(Case(M.gri_size(0), 2, 1e-6, 34, seed=12), n_params=24)
