@@ -47,19 +47,23 @@ struct AdjLayout {
 };
 enum { MS_RHO = 0, MS_CPM, MS_DCPM, MS_AV, MS_RHOB, MS_CPMB, MS_DCPMB, MS_AVB, MS_TB, MS_SH, MS_N = 16 };
 
-__host__ __device__ inline AdjLayout make_adj_layout(const WsLayout& L, int nS, int nR, int n_tb) {
+// y2, y3 and fs live in the forward workspace (shared memory), after its
+// make_layout part (fwd_size doubles in all); every other array is in the
+// per-CTA adjoint region in global memory, offsets from 0.
+__host__ __device__ inline AdjLayout make_adj_layout(const WsLayout& L, int nS, int nR, int n_tb, int* fwd_size) {
     const int m = nS + 1;
     AdjLayout A;
-    int o = L.size;
-    A.y2 = o; o += m;
-    A.y3 = o; o += m;
+    A.y2 = L.size;
+    A.y3 = L.size + m;
+    A.fs = L.size + 2 * m;            // f at the point being reversed
+    *fwd_size = L.size + 3 * m;
+    int o = 0;
     A.rb = o; o += 4 * m;
     A.kb = o; o += 4 * m;
     A.yb = o; o += m;
     A.fb0 = o; o += m;
     A.fb2 = o; o += m;
     A.fb3 = o; o += m;
-    A.fs = o; o += m;                // f at the point being reversed
     A.Jb = o; o += m * L.ld;
     A.raw = o; o += m * L.ld;
     A.cb = o; o += nS;
@@ -97,42 +101,108 @@ struct AdjArgs {
 // ------------------------------------------------------------------ pieces
 
 // W^T x = b with the factors of W (rows permuted: P W = L U): U^T z = b
-// (forward), L^T v = z (backward, unit diagonal), x[perm[i]] = v[i].
-template <int G, class W>
-__device__ void lu_solve_transposed(const Grp<G>& g, const W& w, int A, int ld, int perm, int m, int b, int x) {
-    g.sync();
-    if (g.lane == 0) {
-        for (int i = 0; i < m; ++i) {
-            double s = w[b + i];
-            for (int j = 0; j < i; ++j) s -= w[A + j * ld + i] * w[x + j];
-            w[x + i] = s / w[A + i * ld + i];
-        }
-        for (int i = m - 2; i >= 0; --i) {
-            double s = w[x + i];
-            for (int j = i + 1; j < m; ++j) s -= w[A + j * ld + i] * w[x + j];
-            w[x + i] = s;
+// (forward substitution), L^T v = z (backward, unit diagonal), x[perm[i]] =
+// v[i]. One warp, R rows per lane (lane l holds rows l + 32 u), column by
+// column with the pivot value broadcast by a shuffle; the entries used at
+// step j are row j of the factors (contiguous). m <= 32 R.
+template <int R, class W>
+__device__ void lu_solve_transposed_warp(const W& w, const WsC& wa, int A, int ld, int perm, int m, int b, int x) {
+    const int lane = threadIdx.x & 31;
+    double z[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+        const int i = 32 * u + lane;
+        z[u] = i < m ? wa[b + i] : 0.0;
+    }
+    // U^T z = b: z_j = b_j / U[j][j], then b_i -= U[j][i] z_j for i > j
+    for (int j = 0; j < m; ++j) {
+        const int t = j >> 5, l = j & 31;
+        double zt = z[0];
+#pragma unroll
+        for (int u = 1; u < R; ++u)
+            if (u == t) zt = z[u];
+        const double zj = __shfl_sync(0xffffffffu, zt, l) / w[A + j * ld + j];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int i = 32 * u + lane;
+            if (i == j) z[u] = zj;
+            if (i > j && i < m) z[u] -= w[A + j * ld + i] * zj;
         }
     }
+    // L^T v = z: v_j final, then z_i -= L[j][i] v_j for i < j (descending j)
+    for (int j = m - 1; j >= 0; --j) {
+        const int t = j >> 5, l = j & 31;
+        double zt = z[0];
+#pragma unroll
+        for (int u = 1; u < R; ++u)
+            if (u == t) zt = z[u];
+        const double vj = __shfl_sync(0xffffffffu, zt, l);
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int i = 32 * u + lane;
+            if (i < j) z[u] -= w[A + j * ld + i] * vj;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+        const int i = 32 * u + lane;
+        if (i < m) wa[x + w.ip(perm + i)] = z[u];
+    }
+}
+
+template <int G, class W>
+__device__ void lu_solve_transposed(const Grp<G>& g, const W& w, const WsC& wa, int A, int ld, int perm, int m, int b,
+                                    int x) {
     g.sync();
-    // x[perm[i]] = v[i]: through the b buffer
-    for (int i = g.lane; i < m; i += G) w[b + i] = w[x + i];
+    if (threadIdx.x < 32) {
+        if (m <= 64)
+            lu_solve_transposed_warp<2>(w, wa, A, ld, perm, m, b, x);
+        else if (m <= 128)
+            lu_solve_transposed_warp<4>(w, wa, A, ld, perm, m, b, x);
+        else
+            lu_solve_transposed_warp<10>(w, wa, A, ld, perm, m, b, x);
+    }
     g.sync();
-    for (int i = g.lane; i < m; i += G) w[x + w.ip(perm + i)] = w[b + i];
-    g.sync();
+}
+
+// stream_gather with the sources in one workspace and the results in another
+template <int G, class WS, class WD>
+__device__ __forceinline__ void stream_gather2(const Grp<G>& g, const Stream& st, const WS& ws, int src, const WD& wd,
+                                               int dst) {
+    constexpr int U = 8;
+    const int4* r = reinterpret_cast<const int4*>(st.rec) + g.lane;
+    const int len = st.len;
+    double acc = 0.0;
+    for (int k0 = 0; k0 < len; k0 += U) {
+        int4 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = (k0 + u < len) ? __ldg(r + (size_t)(k0 + u) * G) : make_int4(-1, -1, 0, 0);
+        double x[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) x[u] = v[u].y >= 0 ? ws[src + v[u].y] : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (v[u].y >= 0) acc += __hiloint2double(v[u].w, v[u].z) * x[u];
+            if (v[u].x >= 0) {
+                wd[dst + v[u].x] = acc;
+                acc = 0.0;
+            }
+        }
+    }
 }
 
 // Mixture of the state at y (gpuMixture.H:33-121), as mixture() computes it,
 // with its scalars kept in ms[]: rhoM, CpM, dCpMdT, alphav.
 template <int G, class W>
-__device__ void adj_mixture(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const AdjLayout& A,
+__device__ void adj_mixture(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L, const AdjLayout& A,
                             int y_off, double p) {
     double rhoM, CpM, dCpMdT, alphav;
     mixture(g, M, w, L, y_off, p, true, &rhoM, &CpM, &dCpMdT, &alphav);
     if (g.lane == 0) {
-        w[A.ms + MS_RHO] = rhoM;
-        w[A.ms + MS_CPM] = CpM;
-        w[A.ms + MS_DCPM] = dCpMdT;
-        w[A.ms + MS_AV] = alphav;
+        wa[A.ms + MS_RHO] = rhoM;
+        wa[A.ms + MS_CPM] = CpM;
+        wa[A.ms + MS_DCPM] = dCpMdT;
+        wa[A.ms + MS_AV] = alphav;
     }
     g.sync();
 }
@@ -140,12 +210,12 @@ __device__ void adj_mixture(const Grp<G>& g, const DevMech& M, const W& w, const
 // Reverse of mixture(): given the adjoints of c (cb), Cp, Ha, rhoM/W, v (vb)
 // and of the scalars (ms), adds the gradient w.r.t. the state y to ybar.
 template <int G, class W>
-__device__ void adj_mixture_reverse(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
+__device__ void adj_mixture_reverse(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L,
                                     const AdjLayout& A, int y_off, double p, int ybar) {
     const int nS = M.nS;
     const double T = w[y_off + nS];
     const double invT = 1.0 / T;
-    const double rhoM = w[A.ms + MS_RHO];
+    const double rhoM = wa[A.ms + MS_RHO];
     // sums of the forward that the reverse needs
     double s_av = 0.0;
     for (int i = g.lane; i < nS; i += G) {
@@ -157,12 +227,12 @@ __device__ void adj_mixture_reverse(const Grp<G>& g, const DevMech& M, const W& 
     double rhoMb_l = 0.0;
     for (int i = g.lane; i < nS; i += G) {
         const double yi = fmax(w[y_off + i], 0.0);
-        rhoMb_l += w[A.vb + 2 * nS + i] / ldg(M.W + i) + w[A.cb + i] * (yi / ldg(M.W + i));
+        rhoMb_l += wa[A.vb + 2 * nS + i] / ldg(M.W + i) + wa[A.cb + i] * (yi / ldg(M.W + i));
     }
-    const double rhoMb = w[A.ms + MS_RHOB] + g.sum(rhoMb_l) + w[A.ms + MS_AVB] * s_av;
-    const double s_avb = w[A.ms + MS_AVB] * rhoM;
+    const double rhoMb = wa[A.ms + MS_RHOB] + g.sum(rhoMb_l) + wa[A.ms + MS_AVB] * s_av;
+    const double s_avb = wa[A.ms + MS_AVB] * rhoM;
     const double s_rhob = -rhoMb * rhoM * rhoM;
-    const double CpMb = w[A.ms + MS_CPMB], dCpMb = w[A.ms + MS_DCPMB];
+    const double CpMb = wa[A.ms + MS_CPMB], dCpMb = wa[A.ms + MS_DCPMB];
     double Tb = 0.0, invTb = 0.0;
     for (int i = g.lane; i < nS; i += G) {
         const double Yi = w[y_off + i];
@@ -173,21 +243,21 @@ __device__ void adj_mixture_reverse(const Grp<G>& g, const DevMech& M, const W& 
         const double Cpi = th_Cp(a, T);
         const double dCpi = th_dCpdT(a, T);
         const double d2Cpi = (12.0 * a.a4 * T + 6.0 * a.a3) * T + 2.0 * a.a2;
-        const double yb = s_rhob / rhoi + CpMb * Cpi + w[A.cb + i] * rhoM / ldg(M.W + i) + dCpMb * dCpi +
+        const double yb = s_rhob / rhoi + CpMb * Cpi + wa[A.cb + i] * rhoM / ldg(M.W + i) + dCpMb * dCpi +
                           s_avb * vi * invT;
         double rhoib = -s_rhob * yi / (rhoi * rhoi);
-        const double vb = w[A.vb + 3 * nS + i] + s_avb * yi * invT;
+        const double vb = wa[A.vb + 3 * nS + i] + s_avb * yi * invT;
         rhoib += -vb / (rhoi * rhoi);
         Tb += rhoib * (-rhoi / T);
-        Tb += (w[A.vb + i] + CpMb * yi) * dCpi;  // Cp_i(T)
-        Tb += w[A.vb + nS + i] * Cpi;             // Ha_i(T): dHa/dT = Cp
+        Tb += (wa[A.vb + i] + CpMb * yi) * dCpi;  // Cp_i(T)
+        Tb += wa[A.vb + nS + i] * Cpi;             // Ha_i(T): dHa/dT = Cp
         Tb += dCpMb * yi * d2Cpi;                 // dCp_i/dT(T)
         invTb += s_avb * yi * vi;
-        w[ybar + i] += Yi > 0.0 ? yb : 0.0;
+        wa[ybar + i] += Yi > 0.0 ? yb : 0.0;
     }
     Tb = g.sum(Tb);
     invTb = g.sum(invTb);
-    if (g.lane == 0) w[ybar + nS] += Tb - invTb * invT * invT + w[A.ms + MS_TB];
+    if (g.lane == 0) wa[ybar + nS] += Tb - invTb * invT * invT + wa[A.ms + MS_TB];
     g.sync();
 }
 
@@ -197,7 +267,7 @@ __device__ void adj_mixture_reverse(const Grp<G>& g, const DevMech& M, const W& 
 // per-entry slots (gq), third-body ones to Mb, T to ms[MS_TB] (summed by the
 // caller), parameters to theta_bar (accumulated).
 template <int G, class W>
-__device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const AdjLayout& A,
+__device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L, const AdjLayout& A,
                               int y_off, int rawb, double* theta_bar) {
     const int nS = M.nS;
     const double T = w[y_off + nS];
@@ -207,8 +277,8 @@ __device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, con
         load_rxn(M, q, R);
         // omega_bar = sum over the reaction's species of nu * dN/dt_bar
         double ob = 0.0;
-        for (int e = 0; e < R.nl; ++e) ob -= ldg(M.sst + R.sp_off + e) * w[A.dn + R.idx[0][e]];
-        for (int e = 0; e < R.nr; ++e) ob += ldg(M.sst + R.sp_off + R.nl + e) * w[A.dn + R.idx[1][e]];
+        for (int e = 0; e < R.nl; ++e) ob -= ldg(M.sst + R.sp_off + e) * wa[A.dn + R.idx[0][e]];
+        for (int e = 0; e < R.nr; ++e) ob += ldg(M.sst + R.sp_off + R.nl + e) * wa[A.dn + R.idx[1][e]];
         // the Jacobian terms' weights: ghat[col] = sum over rows s of the
         // reaction of nu_s * rawbar[s][col]
         double gD[2 * kSideInline], gT = 0.0, gE = 0.0;
@@ -240,6 +310,76 @@ __device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, con
 #pragma unroll
             for (int e = kSideInline; e < 2 * kSideInline; ++e) gD[e] = -gD[e];
         }
+        if (rawb < 0 && (R.type == GF_RATE_ARRHENIUS || R.type == GF_RATE_THIRD_BODY_ARRHENIUS)) {
+            // omega only, closed form: with phi = Cf - Cr/Kc, d omega / d kf = phi,
+            // d omega / d c (lhs) = kf dCf/dc, (rhs) = -kr dCr/dc,
+            // d omega / dT = phi dkf/dT + kr Cr dln(Kc)/dT (the ln K cap of
+            // gpuThermo.H:84-85 taken as computed), d kf / d(ln|A|, beta, Ta) =
+            // kf (1, ln T, -1/T), d omega / dM = Ak phi (third body)
+            const double invT = 1.0 / T, logT = ::log(T);
+            const double Ak = R.sA0 * ::exp(fma(R.beta0, logT, R.lnA0) - R.Ta0 * invT);
+            const double Mc = R.tb_row >= 0 ? w[L.Mtb + R.tb_row] : 0.0;
+            const double kf = R.type == GF_RATE_THIRD_BODY_ARRHENIUS ? Mc * Ak : Ak;
+            const double dkfdT = kf * ((R.beta0 + R.Ta0 * invT) * invT);
+            double pw[2][kSideInline], dm[2][kSideInline], C2[2] = {1.0, 1.0};
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const int n = side ? R.nr : R.nl;
+#pragma unroll
+                for (int e = 0; e < kSideInline; ++e) {
+                    pw[side][e] = 1.0;
+                    dm[side][e] = 1.0;
+                    if (e < n) {
+                        const double x = w[L.c + R.idx[side][e]];
+                        pw[side][e] = specie_pow(x, R.iexp[side][e], R.sexp[side][e]);
+                        dm[side][e] = R.sexp[side][e] * specie_pow_m1(x, R.iexp[side][e], R.sexp[side][e]);
+                        C2[side] *= pw[side][e];
+                    }
+                }
+            }
+            double invKc = 1.0, kr = 0.0, dlnK = 0.0, Cr = 0.0;
+            if (!R.irr) {
+                const TCache tc = make_tcache(T);
+                const Poly7 a = reaction_coeffs_at(M, q, T, R.Tcommon);
+                const double Gstd = th_Gstd(a, T, logT);
+                const double arg = -R.Y * Gstd * invT * (1.0 / kRR);
+                double lnK = arg < 600 ? arg : 0.5 * ::log(kVGreat);
+                if (!R.nm_small) lnK += R.nm * tc.lx;
+                invKc = ::exp(-lnK);
+                kr = kf * invKc;
+                Cr = C2[1];
+                if (arg < 600) dlnK = (th_S_pstd(a, T, logT) + Gstd * invT) * R.Y * invT * (1.0 / kRR);
+                if (!R.nm_small) dlnK -= R.nm * invT;
+            }
+            const double phi = C2[0] - Cr * invKc;
+            double gr[2 * kSideInline];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const int n = side ? R.nr : R.nl;
+#pragma unroll
+                for (int j = 0; j < kSideInline; ++j) {
+                    double d = 0.0;
+                    if (j < n && !(side && R.irr)) {
+                        d = 1.0;
+#pragma unroll
+                        for (int i = 0; i < kSideInline; ++i)
+                            if (i < n) d *= (i == j) ? dm[side][i] : pw[side][i];
+                        d *= side ? -kr : kf;
+                    }
+                    gr[side * kSideInline + j] = ob * d;
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < 2 * kSideInline; ++e) wa[A.gq + q * 2 * kSideInline + e] = gr[e];
+            if (R.tb_row >= 0) wa[A.Mb + R.tb_row] = ob * Ak * phi;
+            Tb += ob * (phi * dkfdT + kr * Cr * dlnK);
+            const int r = ldg(M.r_of_q + q);
+            const double gk = ob * phi * kf;
+            theta_bar[3 * r] += gk;
+            theta_bar[3 * r + 1] += gk * logT;
+            theta_bar[3 * r + 2] += -gk * invT;
+            continue;
+        }
         // dual evaluation
         using D = Dual<kAdjK>;
         D c[2 * kSideInline];
@@ -266,8 +406,8 @@ __device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, con
             gr[k] = h;
         }
 #pragma unroll
-        for (int e = 0; e < 2 * kSideInline; ++e) w[A.gq + q * 2 * kSideInline + e] = gr[e];
-        if (R.tb_row >= 0) w[A.Mb + R.tb_row] = gr[kSeedM];
+        for (int e = 0; e < 2 * kSideInline; ++e) wa[A.gq + q * 2 * kSideInline + e] = gr[e];
+        if (R.tb_row >= 0) wa[A.Mb + R.tb_row] = gr[kSeedM];
         Tb += gr[kSeedT];
         const int r = ldg(M.r_of_q + q);
         theta_bar[3 * r] += gr[kSeedLnA];
@@ -275,20 +415,20 @@ __device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, con
         theta_bar[3 * r + 2] += gr[kSeedTa];
     }
     Tb = g.sum(Tb);
-    if (g.lane == 0) w[A.ms + MS_TB] += Tb;
+    if (g.lane == 0) wa[A.ms + MS_TB] += Tb;
     g.sync();
 }
 
 // Concentration adjoints: the per-entry slots gathered per species (stream),
 // plus the third-body terms c_bar[i] += sum_t Mbar[t] eff[t][i].
 template <int G, class W>
-__device__ void adj_gather_c(const Grp<G>& g, const DevMech& M, const W& w, const AdjLayout& A) {
-    stream_gather(g, M.cst[log2_group(G)], w, A.gq, A.dd);
+__device__ void adj_gather_c(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const AdjLayout& A) {
+    stream_gather(g, M.cst[log2_group(G)], wa, A.gq, A.dd);
     g.sync();
     for (int i = g.lane; i < M.nS; i += G) {
-        double acc = w[A.cb + i] + w[A.dd + i];
-        for (int t = 0; t < M.n_tb; ++t) acc += w[A.Mb + t] * ldg(M.eff + (size_t)t * M.nS + i);
-        w[A.cb + i] = acc;
+        double acc = wa[A.cb + i] + wa[A.dd + i];
+        for (int t = 0; t < M.n_tb; ++t) acc += wa[A.Mb + t] * ldg(M.eff + (size_t)t * M.nS + i);
+        wa[A.cb + i] = acc;
     }
     g.sync();
 }
@@ -297,102 +437,106 @@ __device__ void adj_gather_c(const Grp<G>& g, const DevMech& M, const W& w, cons
 // (m) at the point whose f is in fs: dN/dt adjoints to dn, and the adjoints
 // of Ha, CpM, rhoM added to vb / ms.
 template <int G, class W>
-__device__ void adj_rhs_assembly(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
+__device__ void adj_rhs_assembly(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L,
                                  const AdjLayout& A, int fbar) {
     const int nS = M.nS;
-    const double rhoM = w[A.ms + MS_RHO], CpM = w[A.ms + MS_CPM];
+    const double rhoM = wa[A.ms + MS_RHO], CpM = wa[A.ms + MS_CPM];
     const double dTdt = w[A.fs + nS];
-    const double dTb = w[fbar + nS];
+    const double dTb = wa[fbar + nS];
     const double shb = -dTb / CpM;
     double rhoMb = 0.0;
     for (int s = g.lane; s < nS; s += G) {
         const double dYdt = w[A.fs + s];
         const double Wr = ldg(M.W + s) / rhoM;
-        const double dYb = w[fbar + s] + shb * w[L.Ha + s];
-        w[A.vb + nS + s] += shb * dYdt;
-        w[A.dn + s] = dYb * Wr;
+        const double dYb = wa[fbar + s] + shb * w[L.Ha + s];
+        wa[A.vb + nS + s] += shb * dYdt;
+        wa[A.dn + s] = dYb * Wr;
         rhoMb += dYb * (dYdt / Wr) * (-ldg(M.W + s) / (rhoM * rhoM));
     }
     rhoMb = g.sum(rhoMb);
     if (g.lane == 0) {
         // dT/dt = -sh / CpM, sh = sum dY/dt Ha  ->  d/dCpM = -dT/dt / CpM
-        w[A.ms + MS_CPMB] += dTb * (-dTdt / CpM);
-        w[A.ms + MS_RHOB] += rhoMb;
+        wa[A.ms + MS_CPMB] += dTb * (-dTdt / CpM);
+        wa[A.ms + MS_RHOB] += rhoMb;
     }
     g.sync();
 }
 
 template <int G, class W>
-__device__ void adj_clear_point(const Grp<G>& g, const DevMech& M, const W& w, const AdjLayout& A) {
-    for (int i = g.lane; i < 4 * M.nS; i += G) w[A.vb + i] = 0.0;
-    for (int i = g.lane; i < M.nS; i += G) w[A.cb + i] = 0.0;
+__device__ void adj_clear_point(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const AdjLayout& A) {
+    for (int i = g.lane; i < 4 * M.nS; i += G) wa[A.vb + i] = 0.0;
+    for (int i = g.lane; i < M.nS; i += G) wa[A.cb + i] = 0.0;
     for (int i = g.lane; i < MS_N; i += G)
-        if (i >= MS_RHOB) w[A.ms + i] = 0.0;
+        if (i >= MS_RHOB) wa[A.ms + i] = 0.0;
     g.sync();
 }
 
 // ybar += (df/dy)^T fbar at the point y (no Jacobian term)
 template <int G, class W>
-__device__ void adj_vjp_f(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const AdjLayout& A,
+__device__ void adj_vjp_f(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L, const AdjLayout& A,
                           int y_off, double p, int fbar, int ybar, double* theta_bar) {
     derivatives(g, M, w, L, y_off, p, A.fs);  // f, c, Ha and the third-body concentrations at y
-    adj_mixture(g, M, w, L, A, y_off, p);     // + Cp, v, rhoM/W and the scalars
-    adj_clear_point(g, M, w, A);
-    adj_rhs_assembly(g, M, w, L, A, fbar);
-    adj_reactions(g, M, w, L, A, y_off, -1, theta_bar);
-    adj_gather_c(g, M, w, A);
-    adj_mixture_reverse(g, M, w, L, A, y_off, p, ybar);
+    adj_mixture(g, M, w, wa, L, A, y_off, p);     // + Cp, v, rhoM/W and the scalars
+    adj_clear_point(g, M, w, wa, A);
+    adj_rhs_assembly(g, M, w, wa, L, A, fbar);
+    {
+        GF_PH_BEGIN(g)
+        adj_reactions(g, M, w, wa, L, A, y_off, -1, theta_bar);
+        GF_PH_END(g, PH_ADJ_RXN)
+    }
+    adj_gather_c(g, M, w, wa, A);
+    adj_mixture_reverse(g, M, w, wa, L, A, y_off, p, ybar);
 }
 
 // Jacobian term at y0 together with the VJP of f at y0: Jbar (A.Jb) pulled
 // back through the T row and the conversion to the raw entries (into L.J),
 // the adjoints of the mixture quantities, and dfdx_bar added to fbar.
 template <int G, class W>
-__device__ void adj_jacobian_term(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
+__device__ void adj_jacobian_term(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L,
                                   const AdjLayout& A, int y_off, double p, int fbar, int ybar, double* theta_bar) {
     const int nS = M.nS, ld = L.ld;
     // forward: converted J (L.J), dfdx, the Jacobian terms (stage), then the raw entries
     if (g.lane == 0) w[L.scal + S_KCACHE_T] = -1.0;
     g.sync();
     jacobian(g, M, w, L, y_off, p, false);
-    stream_gather(g, M.jst[log2_group(G)], w, L.stage, A.raw);
+    stream_gather2(g, M.jst[log2_group(G)], w, L.stage, wa, A.raw);
     derivatives(g, M, w, L, y_off, p, A.fs);
-    adj_mixture(g, M, w, L, A, y_off, p);
-    adj_clear_point(g, M, w, A);
-    const double CpM = w[A.ms + MS_CPM], rhoM = w[A.ms + MS_RHO], alphav = w[A.ms + MS_AV],
-                 dCpMdT = w[A.ms + MS_DCPM];
+    adj_mixture(g, M, w, wa, L, A, y_off, p);
+    adj_clear_point(g, M, w, wa, A);
+    const double CpM = wa[A.ms + MS_CPM], rhoM = wa[A.ms + MS_RHO], alphav = wa[A.ms + MS_AV],
+                 dCpMdT = wa[A.ms + MS_DCPM];
     const double dTdt = w[L.dfdx + nS];
     // (a) T row: J[nS][i] = (-sum_j J[j][i] Ha_j - Cp_i dTdt) / CpM (i < nS) and
     //     J[nS][nS] = (-sum_i (dfdx_i Cp_i + J[i][nS] Ha_i) - dTdt dCpMdT) / CpM
     double CpMb = 0.0, dTdtb = 0.0;
     for (int i = g.lane; i < nS; i += G) {
-        const double Jb = w[A.Jb + nS * ld + i];
+        const double Jb = wa[A.Jb + nS * ld + i];
         const double ab = Jb / CpM;
-        w[A.ab + i] = ab;
+        wa[A.ab + i] = ab;
         CpMb += -Jb * w[L.J + nS * ld + i] / CpM;
-        w[A.vb + i] += -ab * dTdt;  // Cp_i
+        wa[A.vb + i] += -ab * dTdt;  // Cp_i
         dTdtb += -ab * w[L.Cp + i];
-        for (int j = 0; j < nS; ++j) w[A.Jb + j * ld + i] += -ab * w[L.Ha + j];
+        for (int j = 0; j < nS; ++j) wa[A.Jb + j * ld + i] += -ab * w[L.Ha + j];
     }
     CpMb = g.sum(CpMb);
     dTdtb = g.sum(dTdtb);
-    const double JbTT = w[A.Jb + nS * ld + nS];
+    const double JbTT = wa[A.Jb + nS * ld + nS];
     const double bb = JbTT / CpM;
     if (g.lane == 0) {
-        w[A.ms + MS_CPMB] += CpMb - JbTT * w[L.J + nS * ld + nS] / CpM;
-        w[A.ms + MS_DCPMB] += -bb * dTdt;
-        w[fbar + nS] += dTdtb - bb * dCpMdT;
+        wa[A.ms + MS_CPMB] += CpMb - JbTT * w[L.J + nS * ld + nS] / CpM;
+        wa[A.ms + MS_DCPMB] += -bb * dTdt;
+        wa[fbar + nS] += dTdtb - bb * dCpMdT;
     }
     g.sync();
     // Ha_j adjoint: sum_i -ab_i J[j][i] - bb J[j][nS]; Cp_i, dfdx_i from the TT entry
     for (int j = g.lane; j < nS; j += G) {
         double acc = 0.0;
-        for (int i = 0; i < nS; ++i) acc += -w[A.ab + i] * w[L.J + j * ld + i];
+        for (int i = 0; i < nS; ++i) acc += -wa[A.ab + i] * w[L.J + j * ld + i];
         acc += -bb * w[L.J + j * ld + nS];
-        w[A.vb + nS + j] += acc;
-        w[A.vb + j] += -bb * w[L.dfdx + j];
-        w[fbar + j] += -bb * w[L.Cp + j];
-        w[A.Jb + j * ld + nS] += -bb * w[L.Ha + j];
+        wa[A.vb + nS + j] += acc;
+        wa[A.vb + j] += -bb * w[L.dfdx + j];
+        wa[fbar + j] += -bb * w[L.Cp + j];
+        wa[A.Jb + j * ld + nS] += -bb * w[L.Ha + j];
     }
     g.sync();
     // (b) conversion rows: J[s][c] = Wr_s raw[s][c] rW_c + rhoM v_c dfdx_s,
@@ -402,16 +546,16 @@ __device__ void adj_jacobian_term(const Grp<G>& g, const DevMech& M, const W& w,
         const double Wr = ldg(M.W + s) / rhoM;
         const double dfs = w[L.dfdx + s];
         const int row = A.raw + s * ld, brow = A.Jb + s * ld;
-        double ddN = w[row + nS];
-        for (int c = 0; c < nS; ++c) ddN -= w[row + c] * w[L.c + c] * alphav;
-        const double JbT = w[brow + nS];
+        double ddN = wa[row + nS];
+        for (int c = 0; c < nS; ++c) ddN -= wa[row + c] * w[L.c + c] * alphav;
+        const double JbT = wa[brow + nS];
         const double ddNb = JbT * Wr;
         double Wrb = JbT * ddN;
         avb += JbT * dfs;
         double dfsb = JbT * alphav;
         for (int c = 0; c < nS; ++c) {
-            const double Jb = w[brow + c];
-            const double raw = w[row + c];
+            const double Jb = wa[brow + c];
+            const double raw = wa[row + c];
             Wrb += Jb * raw * w[L.rhoMbyW + c];
             rhoMb += Jb * w[L.vj + c] * dfs;
             dfsb += Jb * rhoM * w[L.vj + c];
@@ -419,85 +563,101 @@ __device__ void adj_jacobian_term(const Grp<G>& g, const DevMech& M, const W& w,
             w[L.J + s * ld + c] = Jb * Wr * w[L.rhoMbyW + c] - ddNb * w[L.c + c] * alphav;  // raw_bar
         }
         w[L.J + s * ld + nS] = ddNb;
-        w[A.dd + s] = ddNb;
+        wa[A.dd + s] = ddNb;
         rhoMb += -Wrb * ldg(M.W + s) / (rhoM * rhoM);
-        w[fbar + s] += dfsb;
+        wa[fbar + s] += dfsb;
     }
     avb = g.sum(avb);
     rhoMb = g.sum(rhoMb);
     if (g.lane == 0) {
-        w[A.ms + MS_AVB] += avb;
-        w[A.ms + MS_RHOB] += rhoMb;
+        wa[A.ms + MS_AVB] += avb;
+        wa[A.ms + MS_RHOB] += rhoMb;
     }
     g.sync();
     // (c) columns: rhoM/W_c, v_c and c_c adjoints
     for (int c = g.lane; c < nS; c += G) {
         double rWb = 0.0, vb = 0.0, cb = 0.0;
         for (int s = 0; s < nS; ++s) {
-            const double Jb = w[A.Jb + s * ld + c];
-            const double raw = w[A.raw + s * ld + c];
+            const double Jb = wa[A.Jb + s * ld + c];
+            const double raw = wa[A.raw + s * ld + c];
             rWb += Jb * (ldg(M.W + s) / rhoM) * raw;
             vb += Jb * rhoM * w[L.dfdx + s];
-            cb += -w[A.dd + s] * raw * alphav;
+            cb += -wa[A.dd + s] * raw * alphav;
         }
-        w[A.vb + 2 * nS + c] += rWb;
-        w[A.vb + 3 * nS + c] += vb;
-        w[A.cb + c] += cb;
+        wa[A.vb + 2 * nS + c] += rWb;
+        wa[A.vb + 3 * nS + c] += vb;
+        wa[A.cb + c] += cb;
     }
     g.sync();
     // the VJP of f at y0 with the completed fbar, the raw terms' pullback, and
     // the mixture reverse for all of it
-    adj_rhs_assembly(g, M, w, L, A, fbar);
-    adj_reactions(g, M, w, L, A, y_off, L.J, theta_bar);
+    adj_rhs_assembly(g, M, w, wa, L, A, fbar);
+    {
+        GF_PH_BEGIN(g)
+        adj_reactions(g, M, w, wa, L, A, y_off, L.J, theta_bar);
+        GF_PH_END(g, PH_ADJ_RXN)
+    }
     // third-body concentrations: the stage pass left Mtb from the Jacobian's
     // mixture, the same state
-    adj_gather_c(g, M, w, A);
-    adj_mixture_reverse(g, M, w, L, A, y_off, p, ybar);
+    adj_gather_c(g, M, w, wa, A);
+    adj_mixture_reverse(g, M, w, wa, L, A, y_off, p, ybar);
 }
 
 // One recorded step in reverse: ybar (A.yb) holds the adjoint of the step's
 // end state on entry and of its start state (L.y0) on exit.
 template <int G, class W>
-__device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const AdjLayout& A,
+__device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L, const AdjLayout& A,
                          const RosCoeffs& C, const OdeParams& o, double p, double h, double* theta_bar) {
     const int m = M.m, ld = L.ld;
     // recompute the attempt (stages kept: k_i, y2, y3; LU factors in L.J)
     if (g.lane == 0) w[L.scal + S_KCACHE_T] = -1.0;
     g.sync();
-    derivatives(g, M, w, L, L.y0, p, L.dydx0);
-    ros_attempt(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3);
+    {
+        GF_PH_BEGIN(g)
+        derivatives(g, M, w, L, L.y0, p, L.dydx0);
+        ros_attempt(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3);
+        GF_PH_END(g, PH_ADJ_RECOMPUTE)
+    }
     // kbar_i = b_i ybar; the ybar of y1 = y0 + sum b_i k_i flows to y0 unchanged
     const double bc[4] = {C.b1, C.b2, C.b3, C.b4};
     for (int i = g.lane; i < m; i += G) {
-        for (int st = 0; st < C.s; ++st) w[A.kb + st * m + i] = bc[st] * w[A.yb + i];
-        w[A.fb0 + i] = 0.0;
-        w[A.fb2 + i] = 0.0;
-        w[A.fb3 + i] = 0.0;
+        for (int st = 0; st < C.s; ++st) wa[A.kb + st * m + i] = bc[st] * wa[A.yb + i];
+        wa[A.fb0 + i] = 0.0;
+        wa[A.fb2 + i] = 0.0;
+        wa[A.fb3 + i] = 0.0;
     }
     g.sync();
     for (int st = C.s - 1; st >= 0; --st) {
         const int rb = A.rb + st * m;
-        lu_solve_transposed(g, w, L.J, ld, L.perm, m, A.kb + st * m, rb);
+        {
+            GF_PH_BEGIN(g)
+            lu_solve_transposed(g, w, wa, L.J, ld, L.perm, m, A.kb + st * m, rb);
+            GF_PH_END(g, PH_ADJ_TSOLVE)
+        }
         const int fsrc = st == 0 ? A.fb0 : (st == 1 || C.s == 3 ? A.fb2 : A.fb3);
         const double hd = h * ros_d(C, st);
         for (int i = g.lane; i < m; i += G) {
-            const double r = w[rb + i];
-            w[fsrc + i] += r;
-            w[A.fb0 + i] += hd * r;  // dfdx = f(y0)
-            for (int j = 0; j < st; ++j) w[A.kb + j * m + i] += (ros_c(C, st, j) / h) * r;
+            const double r = wa[rb + i];
+            wa[fsrc + i] += r;
+            wa[A.fb0 + i] += hd * r;  // dfdx = f(y0)
+            for (int j = 0; j < st; ++j) wa[A.kb + j * m + i] += (ros_c(C, st, j) / h) * r;
         }
         g.sync();
         if (st == 1 || (st == 2 && C.s == 4)) {
             const int pt = st == 1 ? A.y2 : A.y3;
             const int fb = st == 1 ? A.fb2 : A.fb3;
             // ybar of the stage point: into fs-free scratch (A.ab), then to y0 and k_j
-            for (int i = g.lane; i < m; i += G) w[A.ab + i] = 0.0;
+            for (int i = g.lane; i < m; i += G) wa[A.ab + i] = 0.0;
             g.sync();
-            adj_vjp_f(g, M, w, L, A, pt, p, fb, A.ab, theta_bar);
+            {
+                GF_PH_BEGIN(g)
+                adj_vjp_f(g, M, w, wa, L, A, pt, p, fb, A.ab, theta_bar);
+                GF_PH_END(g, PH_ADJ_VJP)
+            }
             for (int i = g.lane; i < m; i += G) {
-                const double yb = w[A.ab + i];
-                w[A.yb + i] += yb;
-                for (int j = 0; j < st; ++j) w[A.kb + j * m + i] += ros_a(C, st, j) * yb;
+                const double yb = wa[A.ab + i];
+                wa[A.yb + i] += yb;
+                for (int j = 0; j < st; ++j) wa[A.kb + j * m + i] += ros_a(C, st, j) * yb;
             }
             g.sync();
         }
@@ -506,18 +666,25 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
     for (int e = g.lane; e < m * m; e += G) {
         const int a = e / m, b = e % m;
         double acc = 0.0;
-        for (int st = 0; st < C.s; ++st) acc += w[A.rb + st * m + a] * w[L.k1 + st * m + b];
-        w[A.Jb + a * ld + b] = acc;
+        for (int st = 0; st < C.s; ++st) acc += wa[A.rb + st * m + a] * w[L.k1 + st * m + b];
+        wa[A.Jb + a * ld + b] = acc;
     }
     g.sync();
-    adj_jacobian_term(g, M, w, L, A, L.y0, p, A.fb0, A.yb, theta_bar);
+    {
+        GF_PH_BEGIN(g)
+        adj_jacobian_term(g, M, w, wa, L, A, L.y0, p, A.fb0, A.yb, theta_bar);
+        GF_PH_END(g, PH_ADJ_JTERM)
+    }
 }
 
 __global__ void __launch_bounds__(64) adjoint_kernel(const DevMech M, const AdjArgs a) {
+    extern __shared__ double smem[];
     Grp<64> g;
     const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
-    const AdjLayout A = make_adj_layout(L, M.nS, M.nR, M.n_tb);
-    WsC w{a.ws + (size_t)blockIdx.x * a.ws_per_cell};
+    int fwd = 0;
+    const AdjLayout A = make_adj_layout(L, M.nS, M.nR, M.n_tb, &fwd);
+    WsC w{smem};
+    WsC wa{a.ws + (size_t)blockIdx.x * a.ws_per_cell};
     const RosCoeffs C = ros_coeffs(a.ode.solver);
     const int nS = M.nS, m = M.m;
     for (;;) {
@@ -535,7 +702,7 @@ __global__ void __launch_bounds__(64) adjoint_kernel(const DevMech M, const AdjA
         const int N = a.counters[2 * cell];
         // the final clip max(0, Y) (singleCellSolver.H:42-45): gradient passes where Y > 0
         for (int i = g.lane; i < m; i += 64)
-            w[A.yb + i] = (fst == GF_CELL_SKIPPED || i == nS || yfin[i] > 0.0) ? ybr[i] : 0.0;
+            wa[A.yb + i] = (fst == GF_CELL_SKIPPED || i == nS || yfin[i] > 0.0) ? ybr[i] : 0.0;
         int status = fst == GF_CELL_SKIPPED ? GF_CELL_OK : fst;
         if (fst == GF_CELL_OK) {
             for (int k = N - 1; k >= 0; --k) {
@@ -543,11 +710,11 @@ __global__ void __launch_bounds__(64) adjoint_kernel(const DevMech M, const AdjA
                 for (int i = g.lane; i < m; i += 64) w[L.y0 + i] = rec[i];
                 const double h = rec[m];
                 __syncthreads();
-                adj_step(g, M, w, L, A, C, a.ode, p, h, thb);
+                adj_step(g, M, w, wa, L, A, C, a.ode, p, h, thb);
             }
         }
         double* yo = a.Y0bar + (size_t)cell * a.ld_y;
-        for (int i = g.lane; i < m; i += 64) yo[i] = status == GF_CELL_OK ? w[A.yb + i] : 0.0;
+        for (int i = g.lane; i < m; i += 64) yo[i] = status == GF_CELL_OK ? wa[A.yb + i] : 0.0;
         if (g.lane == 0) {
             yo[nS + 1] = 0.0;
             a.status[cell] = status;
@@ -560,12 +727,23 @@ __global__ void adj_reset(unsigned long long* q) { q[0] = 0; }
 
 int adjoint_ws_doubles(const DevMech& M) {
     const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
-    return make_adj_layout(L, M.nS, M.nR, M.n_tb).size;
+    int fwd = 0;
+    return make_adj_layout(L, M.nS, M.nR, M.n_tb, &fwd).size;
 }
 
-int adjoint_blocks_per_sm() {
+static int adjoint_smem_bytes(const DevMech& M) {
+    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
+    int fwd = 0;
+    make_adj_layout(L, M.nS, M.nR, M.n_tb, &fwd);
+    return fwd * (int)sizeof(double);
+}
+
+int adjoint_blocks_per_sm(const DevMech& M) {
+    const int smem = adjoint_smem_bytes(M);
+    if (smem > 227 * 1024) return 0;
+    cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 64, 0) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 64, smem) != cudaSuccess) return 0;
     return per_sm;
 }
 
@@ -594,8 +772,12 @@ int launch_adjoint_cells(const DevMech& M, int n_cells, const double* traj, int 
     a.queue = queue;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     adj_reset<<<1, 1, 0, s>>>(queue);
-    if (n_cells > 0) adjoint_kernel<<<n_blocks, 64, 0, s>>>(M, a);
+    if (n_cells > 0) adjoint_kernel<<<n_blocks, 64, adjoint_smem_bytes(M), s>>>(M, a);
     return (int)cudaGetLastError();
 }
+
+#ifdef GF_PHASE_TIMERS
+int phase_cycles_adj(unsigned long long* out, int reset) { return phase_cycles_local(out, reset); }
+#endif
 
 }  // namespace gf

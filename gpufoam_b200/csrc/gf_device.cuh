@@ -59,7 +59,7 @@ static inline int phase_cycles_local(unsigned long long* out, int reset) {
 #define GF_PH_END(g, k)
 #endif
 enum { PH_MIX = 0, PH_NMPOW, PH_OMEGA, PH_GATHER_RHS, PH_JPARAMS, PH_JROWS, PH_TROW, PH_SHIFT, PH_LU, PH_SOLVE,
-       PH_VEC, PH_ATTEMPT, PH_CELL };
+       PH_ADJ_RXN, PH_ATTEMPT, PH_ADJ_RECOMPUTE, PH_ADJ_TSOLVE, PH_ADJ_VJP, PH_ADJ_JTERM };
 
 // ---------------------------------------------------------------- groups
 

@@ -767,7 +767,7 @@ int gf_adjoint(gf_solver* s, int n_cells, const double* traj, int traj_cap, cons
     if (s->mechs.size() != 1 || ld_y < s->max_neq) return GF_ERR_INVALID_ARGUMENT;
     const gf::DevMech& M = s->dmechs[0];
     if (M.max_side > gf::kSideInline) return GF_ERR_UNSUPPORTED;
-    const int per_sm = gf::adjoint_blocks_per_sm();
+    const int per_sm = gf::adjoint_blocks_per_sm(M);
     if (per_sm < 1) return GF_ERR_CUDA;
     const int blocks = per_sm * gf::device_sm_count();
     const long long wsd = gf::adjoint_ws_doubles(M);

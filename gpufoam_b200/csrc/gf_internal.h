@@ -182,7 +182,7 @@ int launch_adjoint_cells(const DevMech& m, int n_cells, const double* traj, int 
                          const int* fwd_status, const double* Y0, const double* Ynew, const double* Ybar, int ld_y,
                          double* Y0bar, double* theta_bar, int* status, const OdeParams& ode, double* ws,
                          long long ws_per_cell, int n_blocks, unsigned long long* queue, void* stream);
-int adjoint_blocks_per_sm();
+int adjoint_blocks_per_sm(const DevMech& m);
 
 // Device tables of a mechanism object (gf_host.cpp).
 const DevMech* mech_device_tables(const gf_mech* m);

@@ -252,6 +252,7 @@ extern "C" int gf_debug_phase_cycles(unsigned long long* out, int reset) {
     phase_cycles_g32(out, reset);
     phase_cycles_g64(out, reset);
     phase_cycles_g128(out, reset);
+    phase_cycles_adj(out, reset);
     return phase_cycles_g256(out, reset);
 }
 namespace gf {

@@ -91,6 +91,7 @@ int phase_cycles_g32(unsigned long long* out, int reset);
 int phase_cycles_g64(unsigned long long* out, int reset);
 int phase_cycles_g128(unsigned long long* out, int reset);
 int phase_cycles_g256(unsigned long long* out, int reset);
+int phase_cycles_adj(unsigned long long* out, int reset);
 #endif
 
 }  // namespace gf
