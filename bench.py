@@ -295,6 +295,7 @@ def main():
     from gpufoam_b200 import _native as N
     from gpufoam_b200 import evaluator as E
     from gpufoam_b200 import flops as F
+    from gpufoam_b200 import sharding
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -334,8 +335,7 @@ def main():
             launches += 2  # queue reset + the solve kernel
             if world > 1:
                 # the exchange of the step: min over ranks of the new chemistry time step
-                mn = dtc.min().reshape(1)
-                dist.all_reduce(mn, op=dist.ReduceOp.MIN)
+                sharding.global_min_delta_t(float(dtc.min()), device="cuda")
             torch.cuda.synchronize()
             ms.append(e0.elapsed_time(e1))
         torch.cuda.synchronize()

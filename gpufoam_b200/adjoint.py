@@ -127,9 +127,10 @@ class ChemistryStep(torch.autograd.Function):
         dtc = torch.full((Y0.shape[0],), float(deltaTChem0), dtype=torch.float64, device=Y0.device)
         Y1, status, counters = solver.forward(Y0.detach(), deltaT, dtc)
         ctx.solver = solver
+        ctx.theta_device = theta.device
         return Y1
 
     @staticmethod
     def backward(ctx, Ybar):
         Y0bar, thb, status = ctx.solver.backward(Ybar)
-        return Y0bar, thb.to(Ybar.device), None, None, None
+        return Y0bar, thb.to(ctx.theta_device), None, None, None

@@ -140,3 +140,28 @@ def test_adjoint_coverage_mechanism():
 @pytest.mark.gpu
 def test_adjoint_grisize():
     check_case(Case(M.gri_size(0), 2, 1e-6, 34, seed=12), n_params=24)
+
+
+@pytest.mark.gpu
+def test_autograd_function():
+    """ChemistryStep through torch.autograd: loss.backward() fills Y0.grad and
+    theta.grad with the adjoint's gradients."""
+    import torch
+    raw = M.h2_size(0)
+    sol = AD.AdjointSolver(raw, E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4), traj_cap=1024)
+    cells = M.make_cells(raw, 4, seed=3)
+    Y0 = torch.tensor(cells, device="cuda", requires_grad=True)
+    theta = torch.tensor(sol.parameters(), requires_grad=True)
+    wts = torch.as_tensor(np.random.default_rng(2).standard_normal(cells.shape), device="cuda")
+    Y1 = AD.ChemistryStep.apply(Y0, theta, sol, 1e-5, 1e-7)
+    (wts * Y1).sum().backward()
+    assert Y0.grad is not None and theta.grad is not None
+    assert torch.isfinite(Y0.grad).all() and torch.isfinite(theta.grad).all()
+    # the same numbers as the solver's own backward
+    Yb, thb, st = sol.backward(wts)
+    assert torch.equal(Y0.grad, Yb) and np.array_equal(theta.grad.numpy(), thb.cpu().numpy())
+    # a perturbed theta changes the forward (the parameters are live inputs)
+    th2 = theta.detach().clone()
+    th2[0, 0] += 0.5
+    Y2 = AD.ChemistryStep.apply(Y0.detach(), th2, sol, 1e-5, 1e-7)
+    assert not torch.equal(Y1.detach(), Y2)
