@@ -82,6 +82,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint measurement (4096 GRI-size cells, deltaT 1e-4 s)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="print only the adjoint measurement (one JSON line) and exit")
+    ap.add_argument("--adjoint-cells", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -207,7 +210,7 @@ def cpu_reference_rate(batch, solver, dT, seconds, nthreads, offset=0):
 ADJOINT = dict(mech="gri", n=4096, dT=1e-4, T=(1100.0, 1600.0))
 
 
-def adjoint_measure(solver_launch, steps):
+def adjoint_measure(solver_launch, steps, n_cells=4096):
     """Forward (plain solve and recording solve) and adjoint sweep times on the
     differentiation workload: 4096 GRI-size cells, T ~ U[1100, 1600] K, deltaT
     1e-4 s (through ignition), Rosenbrock34; loss = seeded weights . final (Y, T).
@@ -217,7 +220,7 @@ def adjoint_measure(solver_launch, steps):
     from gpufoam_b200 import evaluator as E
     from gpufoam_b200 import mechanism as M
     raw = M.gri_size(0)
-    cells = M.make_cells(raw, ADJOINT["n"], seed=4096, T_range=ADJOINT["T"])
+    cells = M.make_cells(raw, n_cells, seed=4096, T_range=ADJOINT["T"])
     ode = E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4)
     sol = AD.AdjointSolver(raw, ode, traj_cap=4096, launch=solver_launch)
     Y0 = torch.as_tensor(cells, device="cuda")
@@ -226,12 +229,12 @@ def adjoint_measure(solver_launch, steps):
     ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     fw, rec, adj = [], [], []
     for k in range(steps + 1):
-        dtc = torch.full((ADJOINT["n"],), DTC0, dtype=torch.float64, device="cuda")
+        dtc = torch.full((n_cells,), DTC0, dtype=torch.float64, device="cuda")
         a0, a1 = ev()
         a0.record()
         sol.solver.solve(Y0, ADJOINT["dT"], dtc, want_status=False, want_counters=False, want_stats=False)
         a1.record()
-        dtc = torch.full((ADJOINT["n"],), DTC0, dtype=torch.float64, device="cuda")
+        dtc = torch.full((n_cells,), DTC0, dtype=torch.float64, device="cuda")
         b0, b1 = ev()
         b0.record()
         Y1, status, counters = sol.forward(Y0, ADJOINT["dT"], dtc)
@@ -248,7 +251,7 @@ def adjoint_measure(solver_launch, steps):
     cnt = counters.cpu().numpy()
     ok = int(((status.cpu().numpy() == 0) & (st.cpu().numpy() == 0)).sum())
     f, r, a = float(np.mean(fw)), float(np.mean(rec)), float(np.mean(adj))
-    return {"workload": "4096 GRI-size cells, T~U[1100,1600] K, deltaT 1e-4 s, Rosenbrock34",
+    return {"workload": f"{n_cells} GRI-size cells, T~U[1100,1600] K, deltaT 1e-4 s, Rosenbrock34",
             "forward_ms": f, "forward_recording_ms": r, "adjoint_ms": a, "adjoint_over_forward": a / f,
             "accepted_steps_per_cell": {"mean": float(cnt[:, 0].mean()), "max": int(cnt[:, 0].max())},
             "cells_ok": ok, "parameters": f"{raw.n_reactions} x (ln|A|, beta, Ta)"}
@@ -263,6 +266,14 @@ def main():
     nthreads = os.cpu_count() or 1
     cfg_desc = {"workload": args.workload, "solver": f"Rosenbrock{args.solver}", "relTol": 1e-4, "absTol": 1e-8,
                 "deltaT": wl["dT"] if "dT_cell" not in wl else f"per cell, log-U{list(wl['dT_cell'])} s"}
+
+    if args.adjoint_only:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"adjoint": adjoint_measure(dict(kind=1, threads_per_cell=128, scratch_in_shared=1,
+                                                          register_budget=1), max(1, args.steps),
+                                                     args.adjoint_cells)}))
+        return
 
     if args.impl == "reference":
         if rank != 0:

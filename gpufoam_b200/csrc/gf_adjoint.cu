@@ -615,7 +615,7 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
     {
         GF_PH_BEGIN(g)
         derivatives(g, M, w, L, L.y0, p, L.dydx0);
-        ros_attempt(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3);
+        ros_attempt<G, W, true>(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3);
         GF_PH_END(g, PH_ADJ_RECOMPUTE)
     }
     // kbar_i = b_i ybar; the ybar of y1 = y0 + sum b_i k_i flows to y0 unchanged
@@ -723,7 +723,36 @@ __global__ void __launch_bounds__(64) adjoint_kernel(const DevMech M, const AdjA
     }
 }
 
+// The recording solve (gf_solve_record): the persistent form with one cell
+// per 128-thread CTA, workspace in shared memory, at most 128 registers, and
+// each accepted step recorded for the sweep.
+__global__ void __launch_bounds__(128, 4) record_kernel(const DevMech M, const LaunchArgs a) {
+    extern __shared__ double smem[];
+    Grp<128> g;
+    for (;;) {
+        long long cell = 0;
+        if (g.lane == 0) cell = (long long)atomicAdd(a.queue, 1ull);
+        cell = g.bcast_ll(cell, 0);
+        if (cell >= a.n_cells) break;
+        process_cell<128, WsC, true>(g, M, WsC{smem}, a, (int)cell);
+    }
+}
+
 __global__ void adj_reset(unsigned long long* q) { q[0] = 0; }
+
+int launch_record(const DevMech& M, const LaunchArgs& a, void* stream) {
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int smem = make_layout(M.nS, M.nR, M.n_slots, M.n_tb).size * (int)sizeof(double);
+    if (smem > 227 * 1024) return (int)cudaErrorInvalidValue;
+    cudaFuncSetAttribute(record_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, record_kernel, 128, smem);
+    if (e != cudaSuccess) return (int)e;
+    if (per_sm < 1) return (int)cudaErrorInvalidConfiguration;
+    launch_epilogue_reset(a.queue, stream);
+    if (a.n_cells > 0) record_kernel<<<per_sm * device_sm_count(), 128, smem, s>>>(M, a);
+    return (int)cudaGetLastError();
+}
 
 int adjoint_ws_doubles(const DevMech& M) {
     const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);

@@ -1557,7 +1557,8 @@ __device__ __forceinline__ double ros_d(const RosCoeffs& C, int i) {
 // solve(y0, dydx0, dx, y, buffer)); returns the normalised error
 // (normaliseError.H:6-29; the p entry contributes 0). y0 is at y0_off, the
 // candidate is written to yt_off.
-template <int G, class W>
+// SAVE (the adjoint sweep): the stage points are kept at save_y2 / save_y3.
+template <int G, class W, bool SAVE = false>
 __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
                               const OdeParams& o, int y0_off, int yt_off, double p, double dx, int save_y2 = -1,
                               int save_y3 = -1) {
@@ -1595,7 +1596,7 @@ __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M,
         const int ki = L.k1 + st * m;
         if (st == 1 || (st == 2 && C.s == 4)) {
             // the stage point (kept at save_y2 / save_y3 when asked: the adjoint sweep)
-            const int pt = (st == 1 && save_y2 >= 0) ? save_y2 : ((st == 2 && save_y3 >= 0) ? save_y3 : yt_off);
+            const int pt = !SAVE ? yt_off : (st == 1 ? save_y2 : (st == 2 ? save_y3 : yt_off));
             for (int i = g.lane; i < m; i += G) {
                 double v = w[y0_off + i];
                 for (int j = 0; j < st; ++j) v += ros_a(C, st, j) * w[L.k1 + j * m + i];
@@ -1652,7 +1653,9 @@ struct CellResult {
 // The state lives at *y_off (swapped with *yt_off on acceptance). Returns a
 // gf_cell_status. maxSteps exhausted: dxTry is left unchanged (the reference
 // returns without writing it).
-template <int G, class W>
+// REC (the adjoint's forward pass): each accepted step's start state and
+// size are recorded at rec (rec_cap steps at most, rec_ld doubles each).
+template <int G, class W, bool REC = false>
 __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const OdeParams& o,
                          const RosCoeffs& C, double xStart, double xEnd, int* y_off, int* yt_off, double p,
                          double* dxTry, int* accepted, int* attempts, double* rec = nullptr, int rec_cap = 0,
@@ -1685,7 +1688,7 @@ __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, cons
             }
         } while (err > 1.0);
         x += dx;
-        if (rec) {
+        if constexpr (REC) {
             // the accepted step's start state and size, for the adjoint sweep
             if (*accepted >= rec_cap) return GF_CELL_MAX_STEPS;
             double* r = rec + (size_t)(*accepted) * rec_ld;
@@ -1719,7 +1722,7 @@ __device__ __forceinline__ unsigned long long dbl_key(double v) {
 // singleCellSolver::operator() (singleCellSolver.H:27-51) with the
 // computeYNew / computeRR epilogue (gpuKernelEvaluator.cu:84-96) fused:
 // RR, the min of deltaTChemNew before clamping, and the clamp.
-template <int G, class W>
+template <int G, class W, bool REC = false>
 __device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, const W& w, const LaunchArgs& a, int cell) {
     const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
     const int nS = M.nS, m = M.m;
@@ -1738,9 +1741,9 @@ __device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, 
         double timeLeft = dT;
         while (timeLeft > kSmall) {
             const double dt = timeLeft;
-            double* rec = a.traj ? a.traj + (size_t)cell * a.traj_cap * a.traj_ld : nullptr;
-            const int st = ode_solve(g, M, w, L, a.ode, C, 0.0, dt, &y_off, &yt_off, p, &dxTry, &accepted, &attempts,
-                                     rec, a.traj_cap, a.traj_ld);
+            double* rec = REC ? a.traj + (size_t)cell * a.traj_cap * a.traj_ld : nullptr;
+            const int st = ode_solve<G, W, REC>(g, M, w, L, a.ode, C, 0.0, dt, &y_off, &yt_off, p, &dxTry, &accepted,
+                                                &attempts, rec, a.traj_cap, a.traj_ld);
             if (st != GF_CELL_OK && status == GF_CELL_OK) status = st;
             if (st == GF_CELL_STEP_UNDERFLOW) break;
             int bad = 0;

@@ -736,25 +736,10 @@ int gf_solve_record(gf_solver* s, int n_cells, double deltaT, const double* Y0, 
     a.traj = traj;
     a.traj_cap = traj_cap;
     a.traj_ld = s->dmechs[0].m + 1;
-    const int wsd = s->max_ws_doubles;
-    int slots = 0;
+    a.ws = nullptr;
     a.ws_slot_stride = 0;
-    if (s->cfg.kind == 0) {
-        slots = n_cells;
-        a.ws_slot_stride = n_cells;
-    } else {
-        int blocks = 0, threads = 0;
-        slots = gf::persistent_slots(s->cfg, wsd * (int)sizeof(double), &blocks, &threads);
-        if (slots <= 0) return GF_ERR_UNSUPPORTED;
-        if (s->cfg.scratch_in_shared) slots = 0;
-    }
-    if (slots > 0) {
-        const int r = ensure_ws(s, (size_t)slots * wsd * sizeof(double));
-        if (r) return r;
-    }
-    a.ws = s->ws;
-    const int ce = gf::launch_cells(s->dmechs.data(), 1, s->cfg, a, wsd, slots, stream);
-    return ce ? cuda_fail((cudaError_t)ce) : GF_OK;
+    const int ce = gf::launch_record(s->dmechs[0], a, stream);
+    return ce ? (ce == (int)cudaErrorInvalidValue ? GF_ERR_UNSUPPORTED : cuda_fail((cudaError_t)ce)) : GF_OK;
 }
 
 // The reverse sweep over a recorded trajectory (gf_adjoint.cu).

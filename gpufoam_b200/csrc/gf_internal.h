@@ -183,6 +183,7 @@ int launch_adjoint_cells(const DevMech& m, int n_cells, const double* traj, int 
                          double* Y0bar, double* theta_bar, int* status, const OdeParams& ode, double* ws,
                          long long ws_per_cell, int n_blocks, unsigned long long* queue, void* stream);
 int adjoint_blocks_per_sm(const DevMech& m);
+int launch_record(const DevMech& m, const LaunchArgs& a, void* stream);
 
 // Device tables of a mechanism object (gf_host.cpp).
 const DevMech* mech_device_tables(const gf_mech* m);
