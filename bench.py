@@ -11,9 +11,11 @@ starting each step from the same states and deltaTChem = 1e-7 s (the
 reference tutorials' initialChemicalTimeStep). Inputs are seeded synthetic
 batches larger than L2 (126 MB) for the GPU workloads.
 
-`value`     persistent work-queue kernel, inputs resident in HBM, CUDA events
+`value`     persistent work-queue kernel, captured once as a CUDA graph and
+            replayed every step; inputs resident in HBM, CUDA events
 `plain`     the one-thread-per-cell kernel on the same batch (the reference's
-            launch model), for the persistent-vs-plain ratio
+            launch model, also replayed from a graph), for the
+            persistent-vs-plain ratio
 `e2e`       GpuKernelEvaluator.computeRR through the C ABI from pinned host
             arrays: H2D of Y/ΔTChem/rho, the solve, D2H of RR/ΔTChem
 `roofline`  FP64 pipe: algorithmic FLOP (gpufoam_b200/flops.py) per launch ÷
@@ -57,6 +59,9 @@ WORKLOADS = {
     "gri-4k": dict(mech="gri", n=4096, dT=1e-6, T=(1000.0, 2500.0)),
     "gri-16k": dict(mech="gri", n=16384, dT=1e-6, T=(1000.0, 2500.0)),
     "gri-bimodal-64k": dict(mech="gri", n=65536, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0))),
+    # the real GRI-Mech 3.0 of the reference's unit tests (53 species, 325
+    # reactions, read from its OpenFOAM dictionaries into tests/golden/foam_gri.npz)
+    "gri30-100k": dict(mech="gri30", n=100_000, dT=1e-6, T=(1000.0, 2500.0)),
 }
 DTC0 = 1e-7
 
@@ -98,6 +103,9 @@ class Batch:
 
 def _mech(name):
     from gpufoam_b200 import mechanism as M
+    if name == "gri30":
+        from tests.test_oracle import fixture_mech, load
+        return fixture_mech(load("foam_gri"))
     return {"h2": M.h2_size, "gri": M.gri_size, "large": M.large}[name](0)
 
 
@@ -326,11 +334,14 @@ def main():
     lib = N.load()
 
     def timed(solver, steps, warmup):
+        """W + K replays of the solve captured as a CUDA graph (queue reset +
+        solve kernel), each timed with CUDA events on the launching stream."""
         stream = torch.cuda.current_stream()
+        counters = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+        graph = solver.capture(Y0, wl["dT"], dtc, Ynew=Ynew, deltaT_cell=dtcell, mech_id=mid, counters=counters)
         for _ in range(warmup):
             dtc.copy_(dtc0)
-            solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, deltaT_cell=dtcell, mech_id=mid, want_status=False,
-                         want_counters=False, want_stats=False)
+            graph.launch(stream)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -340,8 +351,7 @@ def main():
             dtc.copy_(dtc0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            out = solver.solve(Y0, wl["dT"], dtc, Ynew=Ynew, deltaT_cell=dtcell, mech_id=mid, want_status=False,
-                               want_counters=True, want_stats=False)
+            graph.launch(stream)
             e1.record(stream)
             launches += 2  # queue reset + the solve kernel
             if world > 1:
@@ -352,7 +362,8 @@ def main():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        cnt = out["counters"].cpu().numpy()
+        cnt = counters.cpu().numpy()
+        graph.close()
         return ms, cnt, launches
 
     def flop_of(cnt):

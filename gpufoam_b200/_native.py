@@ -29,7 +29,8 @@ EXPORTS = [
     "gf_solver_create", "gf_solver_destroy", "gf_solver_set_launch", "gf_solver_get_launch", "gf_solve",
     "gf_compute_rr", "gf_compute_ynew", "gf_rates", "gf_jacobian", "gf_lu_decompose", "gf_lu_backsubstitute",
     "gf_strerror", "gf_abi_version", "gf_last_cuda_error", "gf_measure_fp64_peak", "gf_solve_noalloc",
-    "gf_solve_record", "gf_adjoint",
+    "gf_solve_record", "gf_adjoint", "gf_solve_graph_create", "gf_solve_graph_set_delta_t",
+    "gf_solve_graph_launch", "gf_solve_graph_stats", "gf_solve_graph_destroy",
 ]
 
 
@@ -129,6 +130,12 @@ def load() -> C.CDLL:
                                      P(GfStats), vp]
     lib.gf_solve_record.argtypes = [vp, ip, dp, vp, ip, vp, vp, vp, vp, vp, ip, vp]
     lib.gf_adjoint.argtypes = [vp, ip, vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, vp, vp]
+    lib.gf_solve_graph_create.argtypes = [vp, ip, dp, vp, dp, vp, vp, vp, ip, vp, vp, vp, ip, vp, vp, P(vp)]
+    lib.gf_solve_graph_set_delta_t.argtypes = [vp, dp]
+    lib.gf_solve_graph_launch.argtypes = [vp, vp]
+    lib.gf_solve_graph_stats.argtypes = [vp, P(GfStats)]
+    lib.gf_solve_graph_destroy.argtypes = [vp]
+    lib.gf_solve_graph_destroy.restype = None
     lib.gf_strerror.argtypes = [ip]
     lib.gf_strerror.restype = C.c_char_p
     lib.gf_abi_version.restype = ip

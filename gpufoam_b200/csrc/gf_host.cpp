@@ -647,66 +647,238 @@ int gf_solver_get_launch(const gf_solver* s, gf_launch_config* cfg) {
     return GF_OK;
 }
 
-int gf_solve(gf_solver* s, int n_cells, double deltaT, const double* deltaT_cell, double deltaTChemMax,
-             const int* mech_id, const double* rho, const double* Y0, int ld_y, double* Ynew, double* deltaTChem,
-             double* RR, int ld_rr, int* status, int* counters, gf_stats* stats, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// Arguments of one solve, checked; queue and workspace left for the caller.
+int solve_args(const gf_solver* s, int n_cells, double deltaT, const double* deltaT_cell, double deltaTChemMax,
+               const int* mech_id, const double* rho, const double* Y0, int ld_y, double* Ynew,
+               double* deltaTChem, double* RR, int ld_rr, int* status, int* counters, gf::LaunchArgs* a) {
     if (!s || n_cells < 0 || !deltaTChem || !Y0) return GF_ERR_INVALID_ARGUMENT;
     if (ld_y < s->max_neq) return GF_ERR_INVALID_ARGUMENT;
     if (RR && (!rho || ld_rr < 1)) return GF_ERR_INVALID_ARGUMENT;
     if (!mech_id && s->mechs.size() > 1) return GF_ERR_INVALID_ARGUMENT;
     if (RR && s->mechs.size() == 1 && ld_rr < s->dmechs[0].nS) return GF_ERR_INVALID_ARGUMENT;
+    a->n_cells = n_cells;
+    a->deltaT = deltaT;
+    a->deltaT_cell = deltaT_cell;
+    a->deltaTChemMax = deltaTChemMax;
+    a->mech_id = mech_id;
+    a->rho = rho;
+    a->Y0 = Y0;
+    a->ld_y = ld_y;
+    a->Ynew = Ynew;
+    a->deltaTChem = deltaTChem;
+    a->RR = RR;
+    a->ld_rr = ld_rr;
+    a->status = status;
+    a->counters = counters;
+    a->Treact = s->Treact;
+    a->ode = s->ode;
+    a->queue = nullptr;
+    a->ws = nullptr;
+    a->ws_slot_stride = 0;
+    return GF_OK;
+}
+
+// Workspace slots (cells in flight with their workspace in HBM) of the
+// solver's launch form for n_cells; 0 when the workspaces sit in shared memory.
+int solve_slots(const gf_solver* s, int n_cells, int* slots) {
+    *slots = 0;
+    if (s->cfg.kind == 0) {
+        *slots = n_cells;
+        return GF_OK;
+    }
+    int blocks = 0, threads = 0;
+    const int k = gf::persistent_slots(s->cfg, s->max_ws_doubles * (int)sizeof(double), &blocks, &threads);
+    if (k <= 0) return GF_ERR_UNSUPPORTED;
+    if (!s->cfg.scratch_in_shared) *slots = k;
+    return GF_OK;
+}
+
+double min_delta_t_of(unsigned long long k) {
+    const unsigned long long bits = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+    double mn;
+    std::memcpy(&mn, &bits, 8);
+    return mn;
+}
+
+void stats_of(const unsigned long long* q, int n_cells, gf_stats* stats) {
+    stats->min_delta_t = n_cells > 0 ? min_delta_t_of(q[1]) : 0.0;
+    stats->accepted_steps = (long long)q[2];
+    stats->attempts = (long long)q[3];
+    stats->failed_cells = (long long)q[4];
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf_solve(gf_solver* s, int n_cells, double deltaT, const double* deltaT_cell, double deltaTChemMax,
+             const int* mech_id, const double* rho, const double* Y0, int ld_y, double* Ynew, double* deltaTChem,
+             double* RR, int ld_rr, int* status, int* counters, gf_stats* stats, void* stream) {
     gf::LaunchArgs a;
-    a.n_cells = n_cells;
-    a.deltaT = deltaT;
-    a.deltaT_cell = deltaT_cell;
-    a.deltaTChemMax = deltaTChemMax;
-    a.mech_id = mech_id;
-    a.rho = rho;
-    a.Y0 = Y0;
-    a.ld_y = ld_y;
-    a.Ynew = Ynew;
-    a.deltaTChem = deltaTChem;
-    a.RR = RR;
-    a.ld_rr = ld_rr;
-    a.status = status;
-    a.counters = counters;
-    a.Treact = s->Treact;
-    a.ode = s->ode;
-    a.queue = s->queue;
-    a.ws = nullptr;
-    a.ws_slot_stride = 0;
+    int r = solve_args(s, n_cells, deltaT, deltaT_cell, deltaTChemMax, mech_id, rho, Y0, ld_y, Ynew, deltaTChem,
+                       RR, ld_rr, status, counters, &a);
+    if (r) return r;
     const int wsd = s->max_ws_doubles;
     int slots = 0;
-    if (s->cfg.kind == 0) {
-        slots = n_cells;
-        a.ws_slot_stride = n_cells;
-    } else {
-        int blocks = 0, threads = 0;
-        slots = gf::persistent_slots(s->cfg, wsd * (int)sizeof(double), &blocks, &threads);
-        if (slots <= 0) return GF_ERR_UNSUPPORTED;
-        if (s->cfg.scratch_in_shared) slots = 0;
-    }
-    if (slots > 0) {
-        const int r = ensure_ws(s, (size_t)slots * wsd * sizeof(double));
-        if (r) return r;
-    }
+    if ((r = solve_slots(s, n_cells, &slots))) return r;
+    if (slots > 0 && (r = ensure_ws(s, (size_t)slots * wsd * sizeof(double)))) return r;
+    a.queue = s->queue;
     a.ws = s->ws;
+    a.ws_slot_stride = s->cfg.kind == 0 ? n_cells : 0;
     const int ce = gf::launch_cells(s->dmechs.data(), (int)s->dmechs.size(), s->cfg, a, wsd, slots, stream);
     if (ce) return cuda_fail((cudaError_t)ce);
     if (stats) {
         cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
         GF_CUDA(cudaMemcpyAsync(s->queue_host, s->queue, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         GF_CUDA(cudaStreamSynchronize(st));
-        const unsigned long long k = s->queue_host[1];
-        const unsigned long long bits = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
-        double mn;
-        std::memcpy(&mn, &bits, 8);
-        stats->min_delta_t = n_cells > 0 ? mn : 0.0;
-        stats->accepted_steps = (long long)s->queue_host[2];
-        stats->attempts = (long long)s->queue_host[3];
-        stats->failed_cells = (long long)s->queue_host[4];
+        stats_of(s->queue_host, n_cells, stats);
     }
     return GF_OK;
+}
+
+// ---- graph-captured solve -----------------------------------------------------
+
+}  // extern "C"
+
+struct gf_solve_graph {
+    gf_solver* solver = nullptr;
+    gf_launch_config cfg{};                 // the launch form at capture time
+    gf::LaunchArgs args{};
+    int slots = 0;
+    double* ws = nullptr;                   // the graph's own workspaces (HBM form)
+    unsigned long long* queue = nullptr;    // its own work queue and step totals
+    unsigned long long* queue_host = nullptr;
+    cudaStream_t capture = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+// Records the queue reset, the solve kernel and the copy of the step totals
+// to pinned host memory on the graph's private stream.
+int capture_solve(gf_solve_graph* g, cudaGraph_t* out) {
+    gf_solver* s = g->solver;
+    GF_CUDA(cudaStreamBeginCapture(g->capture, cudaStreamCaptureModeRelaxed));
+    int ce = gf::launch_cells(s->dmechs.data(), (int)s->dmechs.size(), g->cfg, g->args, s->max_ws_doubles,
+                              g->slots, g->capture);
+    if (!ce)
+        ce = (int)cudaMemcpyAsync(g->queue_host, g->queue, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                  g->capture);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(g->capture, &graph);
+    if (ce || ee) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_fail(ce ? (cudaError_t)ce : ee);
+    }
+    *out = graph;
+    return GF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf_solve_graph_create(gf_solver* s, int n_cells, double deltaT, const double* deltaT_cell,
+                          double deltaTChemMax, const int* mech_id, const double* rho, const double* Y0, int ld_y,
+                          double* Ynew, double* deltaTChem, double* RR, int ld_rr, int* status, int* counters,
+                          gf_solve_graph** out) {
+    if (!out) return GF_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    gf::LaunchArgs a;
+    int r = solve_args(s, n_cells, deltaT, deltaT_cell, deltaTChemMax, mech_id, rho, Y0, ld_y, Ynew, deltaTChem,
+                       RR, ld_rr, status, counters, &a);
+    if (r) return r;
+    auto* g = new gf_solve_graph;
+    g->solver = s;
+    g->cfg = s->cfg;
+    g->args = a;
+    const size_t wsd = (size_t)s->max_ws_doubles;
+    if ((r = solve_slots(s, n_cells, &g->slots))) {
+        delete g;
+        return r;
+    }
+    cudaError_t e = cudaMalloc(&g->queue, 8 * sizeof(unsigned long long));
+    if (!e) e = cudaMallocHost(&g->queue_host, 8 * sizeof(unsigned long long));
+    if (!e && g->slots > 0) e = cudaMalloc(&g->ws, (size_t)g->slots * wsd * sizeof(double));
+    if (!e) e = cudaStreamCreateWithFlags(&g->capture, cudaStreamNonBlocking);
+    if (e) {
+        gf_solve_graph_destroy(g);
+        return cuda_fail(e);
+    }
+    std::memset(g->queue_host, 0, 8 * sizeof(unsigned long long));
+    g->args.queue = g->queue;
+    g->args.ws = g->ws;
+    g->args.ws_slot_stride = s->cfg.kind == 0 ? n_cells : 0;
+    if ((r = capture_solve(g, &g->graph))) {
+        gf_solve_graph_destroy(g);
+        return r;
+    }
+    e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (e) {
+        gf_solve_graph_destroy(g);
+        return cuda_fail(e);
+    }
+    *out = g;
+    return GF_OK;
+}
+
+int gf_solve_graph_set_delta_t(gf_solve_graph* g, double deltaT) {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    const double old = g->args.deltaT;
+    g->args.deltaT = deltaT;
+    cudaGraph_t graph = nullptr;
+    int r = capture_solve(g, &graph);
+    if (r) {
+        g->args.deltaT = old;
+        return r;
+    }
+    cudaGraphExecUpdateResultInfo info;
+    cudaError_t e = cudaGraphExecUpdate(g->exec, graph, &info);
+    if (e) {
+        // the topology is the same by construction; instantiate afresh if the
+        // driver still refuses the in-place update
+        (void)cudaGetLastError();
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e) {
+            cudaGraphDestroy(graph);
+            g->args.deltaT = old;
+            return cuda_fail(e);
+        }
+        cudaGraphExecDestroy(g->exec);
+        g->exec = exec;
+    }
+    cudaGraphDestroy(g->graph);
+    g->graph = graph;
+    return GF_OK;
+}
+
+int gf_solve_graph_launch(gf_solve_graph* g, void* stream) {
+    if (!g) return GF_ERR_INVALID_ARGUMENT;
+    GF_CUDA(cudaGraphLaunch(g->exec, reinterpret_cast<cudaStream_t>(stream)));
+    return GF_OK;
+}
+
+int gf_solve_graph_stats(const gf_solve_graph* g, gf_stats* stats) {
+    if (!g || !stats) return GF_ERR_INVALID_ARGUMENT;
+    stats_of(g->queue_host, g->args.n_cells, stats);
+    return GF_OK;
+}
+
+void gf_solve_graph_destroy(gf_solve_graph* g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->capture) cudaStreamDestroy(g->capture);
+    cudaFree(g->ws);
+    cudaFree(g->queue);
+    if (g->queue_host) cudaFreeHost(g->queue_host);
+    delete g;
 }
 
 // gf_solve with the trajectory recorded for the adjoint (single mechanism).

@@ -224,9 +224,66 @@ class Solver:
                     stats=dict(accepted=st.accepted_steps, attempts=st.attempts, failed=st.failed_cells,
                                min_delta_t=st.min_delta_t) if want_stats else None)
 
+    def capture(self, Y0, deltaT: float, deltaTChem, deltaTChemMax: float = np.inf, rho=None, deltaT_cell=None,
+                mech_id=None, Ynew=None, RR=None, status=None, counters=None) -> "SolveGraph":
+        """The solve with these tensors captured as a CUDA graph (gf_solve_graph_create):
+        every launch re-reads Y0 / deltaTChem and rewrites Ynew, RR, status, counters in place."""
+        import torch
+        n = int(Y0.shape[0])
+        ld = int(Y0.shape[1])
+        if Ynew is None:
+            Ynew = torch.empty_like(Y0)
+        if rho is not None and RR is None:
+            RR = torch.empty((n, ld), dtype=torch.float64, device=Y0.device)
+        h = C.c_void_p()
+        N.check(self.lib.gf_solve_graph_create(self.handle, n, float(deltaT), _ptr(deltaT_cell), float(deltaTChemMax),
+                                               _ptr(mech_id), _ptr(rho), _ptr(Y0), ld, _ptr(Ynew), _ptr(deltaTChem),
+                                               _ptr(RR), ld if RR is not None else 0, _ptr(status), _ptr(counters),
+                                               C.byref(h)), "gf_solve_graph_create")
+        return SolveGraph(self, h, dict(Y0=Y0, deltaTChem=deltaTChem, rho=rho, deltaT_cell=deltaT_cell,
+                                        mech_id=mech_id, Ynew=Ynew, RR=RR, status=status, counters=counters))
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.gf_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolveGraph:
+    """A captured solve (gf_solve_graph): launch() enqueues it on a stream; the
+    tensors it was captured with stay referenced here for its lifetime."""
+
+    def __init__(self, solver: Solver, handle, tensors):
+        self.solver = solver
+        self.lib = solver.lib
+        self.handle = handle
+        self.tensors = tensors
+
+    def __getitem__(self, name):
+        return self.tensors[name]
+
+    def launch(self, stream=None):
+        N.check(self.lib.gf_solve_graph_launch(self.handle, _stream_ptr(stream)), "gf_solve_graph_launch")
+
+    def set_delta_t(self, deltaT: float):
+        N.check(self.lib.gf_solve_graph_set_delta_t(self.handle, float(deltaT)), "gf_solve_graph_set_delta_t")
+
+    def stats(self) -> dict:
+        """Totals of the last launch (after its stream has synchronized)."""
+        st = N.GfStats()
+        N.check(self.lib.gf_solve_graph_stats(self.handle, C.byref(st)), "gf_solve_graph_stats")
+        return dict(accepted=st.accepted_steps, attempts=st.attempts, failed=st.failed_cells,
+                    min_delta_t=st.min_delta_t)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.gf_solve_graph_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

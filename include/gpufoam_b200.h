@@ -211,6 +211,29 @@ int gf_solve(gf_solver* solver, int n_cells, double deltaT, const double* deltaT
              double* RR, int ld_rr, int* status, int* counters, gf_stats* stats,
              void* stream);
 
+/* ---- graph-captured solve (no counterpart in the reference) ------------- */
+
+typedef struct gf_solve_graph gf_solve_graph;
+
+/* Captures one gf_solve with these arguments (device pointers; no stats) into
+ * an executable CUDA graph: the work-queue reset, the solve kernel and a copy of
+ * the step totals to pinned host memory. The graph owns its workspaces and
+ * queue, so later calls on the solver leave it valid; the solver's launch form
+ * is the one set at capture. Every launch reads and writes the arrays given
+ * here: the caller refills Y0 and deltaTChem in place between launches. The
+ * solver and its mechanisms must outlive the graph. Nothing runs at capture. */
+int gf_solve_graph_create(gf_solver* solver, int n_cells, double deltaT, const double* deltaT_cell,
+                          double deltaTChemMax, const int* mech_id, const double* rho,
+                          const double* Y0, int ld_y, double* Ynew, double* deltaTChem,
+                          double* RR, int ld_rr, int* status, int* counters, gf_solve_graph** out);
+/* New flow time step for later launches (the kernel node is updated in place). */
+int gf_solve_graph_set_delta_t(gf_solve_graph* graph, double deltaT);
+/* Enqueues one solve on stream. */
+int gf_solve_graph_launch(gf_solve_graph* graph, void* stream);
+/* Step totals of the last launch; valid once its stream has synchronized. */
+int gf_solve_graph_stats(const gf_solve_graph* graph, gf_stats* stats);
+void gf_solve_graph_destroy(gf_solve_graph* graph);
+
 /* Host-memory mirror of GpuKernelEvaluator::computeRR (single mechanism):
  * RR [n_cells][nSpecie], deltaTChemNew [n_cells] (clamped), *minDeltaT (before
  * clamping). Copies in and out through pinned staging owned by the solver. */

@@ -8,8 +8,12 @@ compiled in place by oracle/Makefile into oracle/_ref/libgf_ref.so):
 Every expected value in the .npz files below comes from the reference's own
 code (gpuThermo, gpuReaction, gpuODESystem, LUDecompose/LUBacksubstitute,
 gpuRosenbrock12/23/34, odeSolve, singleCellSolver), evaluated on seeded
-synthetic mechanisms and cell states. The raw mechanism is stored with the
-results so that the fixtures do not depend on the generator staying unchanged.
+synthetic mechanisms and cell states, and on the three real mechanisms of the
+reference's unit tests (foam_*.npz, read from their OpenFOAM dictionaries by
+gpufoam_b200.foam_dict). The raw mechanism is stored with the results so that
+the fixtures do not depend on the generator or the reference tree.
+
+    python tests/golden/make_golden.py [case ...]   # default: all cases
 """
 from __future__ import annotations
 
@@ -33,8 +37,39 @@ CASES = [
     ("grisize", M.gri_size, 6, 12, 1e-6),
 ]
 
+# The real mechanisms of the reference's unit tests (OpenFOAM dictionaries
+# embedded as C++ raw strings in gpu_chemistry/unittest/testHelpers/), read by
+# gpufoam_b200.foam_dict, with the reference's own test condition
+# (testHelpers/mechanisms.H:36-107: T = 1000 K, the mechanism's p and three
+# non-zero mass fractions) as state 0.
+REF = os.environ.get("GPUFOAM_REFERENCE", "/root/reference")
+HELPERS = os.path.join(REF, "gpu_chemistry", "unittest", "testHelpers")
+FOAM = [
+    # name, file stem, (species index, Y) of the test condition, p, n states, n cells, deltaT
+    ("foam_h2", "h2", [(0, 0.2), (2, 0.2), (9, 0.6)], 202650.0, 8, 32, 1e-5),
+    ("foam_gri", "gri", [(0, 0.2), (4, 0.5), (47, 0.3)], 1.36789e6, 6, 12, 1e-6),
+    ("foam_yao", "yao", [(44, 0.2), (8, 0.2), (53, 0.6)], 1.36789e6, 6, 12, 1e-6),
+]
 
-def make_case(name, factory, n_states, n_cells, deltaT):
+
+def foam_factory(stem):
+    from gpufoam_b200 import foam_dict
+
+    def make(_seed):
+        return foam_dict.read_mechanism_files(os.path.join(HELPERS, f"{stem}_thermos.h"),
+                                              os.path.join(HELPERS, f"{stem}_reactions.h"), stem)
+    return make
+
+
+def test_condition(mech, fractions, p):
+    y = np.zeros(mech.n_eqns)
+    for i, v in fractions:
+        y[i] = v
+    y[-2], y[-1] = 1000.0, p
+    return y
+
+
+def make_case(name, factory, n_states, n_cells, deltaT, first_state=None):
     mech = factory(0)
     ref = Oracle(mech, "reference")
     fl = flatten(mech)
@@ -44,6 +79,8 @@ def make_case(name, factory, n_states, n_cells, deltaT):
     out["thermo_700"] = ref.thermo_eval(101325.0, 700.0)
     out["thermo_1500"] = ref.thermo_eval(101325.0, 1500.0)
     states = M.make_cells(mech, n_states, seed=11)
+    if first_state is not None:
+        states = np.vstack([first_state[None, :], states[1:]])
     out["states"] = states
     out["reaction_eval"] = np.stack([ref.reaction_eval(s) for s in states[:2]])
     out["dydx"] = ref.derivatives(states)
@@ -56,6 +93,8 @@ def make_case(name, factory, n_states, n_cells, deltaT):
         y, err = ref.attempt(ode_inputs(s), states, out["dydx"], dxs)
         out[f"attempt{s}_y"], out[f"attempt{s}_err"] = y, err
     cells = M.make_cells(mech, n_cells, seed=12)
+    if first_state is not None:
+        cells = np.vstack([first_state[None, :], cells[1:]])
     out["cells"] = cells
     out["deltaT"] = np.array(deltaT)
     out["deltaTChem0"] = np.array(1e-7)
@@ -89,6 +128,14 @@ def make_lu():
 
 
 if __name__ == "__main__":
-    make_lu()
+    only = sys.argv[1:]
+    if not only or "lu" in only:
+        make_lu()
     for case in CASES:
-        make_case(*case)
+        if not only or case[0] in only:
+            make_case(*case)
+    for name, stem, fractions, p, n_states, n_cells, deltaT in FOAM:
+        if only and name not in only:
+            continue
+        factory = foam_factory(stem)
+        make_case(name, factory, n_states, n_cells, deltaT, first_state=test_condition(factory(0), fractions, p))

@@ -143,6 +143,15 @@ def test_adjoint_grisize():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name, deltaT", [("foam_h2", 1e-5), ("foam_gri", 1e-6)])
+def test_adjoint_real_mechanism(name, deltaT):
+    """The reference's real H2 and GRI-Mech 3.0 test mechanisms (read from their
+    OpenFOAM dictionaries, stored in the golden fixtures)."""
+    from tests.test_oracle import fixture_mech, load
+    check_case(Case(fixture_mech(load(name)), 2, deltaT, 34, seed=21), n_params=24)
+
+
+@pytest.mark.gpu
 def test_autograd_function():
     """ChemistryStep through torch.autograd: loss.backward() fills Y0.grad and
     theta.grad with the adjoint's gradients."""

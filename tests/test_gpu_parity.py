@@ -19,7 +19,7 @@ from tests.test_oracle import fixture_mech, load
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["h2size", "coverage", "grisize"]
+CASES = ["h2size", "coverage", "grisize", "foam_h2", "foam_gri", "foam_yao"]
 LAUNCHES = {
     "plain": dict(kind=0),
     "persist-g1-hbm": dict(kind=1, threads_per_cell=1, scratch_in_shared=0),
@@ -224,3 +224,58 @@ def test_mixed_mechanisms_per_cell_dt(torch):
         ref = Oracle(r, "port").cells(ode_inputs(34), Y[sel, :r.n_eqns], 0.0, 1e-7, deltaT_cell=dts[sel])
         assert_states_close(Yg[sel, :r.n_eqns], ref[0], r.n_species, 1e-4, f"mech {k}")
         assert step_count_agreement(cnt[sel], ref[2]) >= 0.97
+
+
+def test_graph_replay_matches_solve(torch):
+    """The captured solve (gf_solve_graph_*) against gf_solve: bit-identical
+    states, steps and totals on every replay; a new flow step through
+    set_delta_t; the graph unaffected by a later change of the solver's launch."""
+    raws = [M.h2_size(0), M.coverage(0)]
+    mechs = [E.Mechanism(r) for r in raws]
+    rng = np.random.default_rng(8)
+    n = 160
+    ld = max(r.n_eqns for r in raws)
+    Y = np.zeros((n, ld))
+    mid = rng.integers(0, 2, n).astype(np.int32)
+    for k, r in enumerate(raws):
+        sel = mid == k
+        Y[sel, :r.n_eqns] = M.make_cells(r, int(sel.sum()), seed=60 + k)
+    s = E.Solver(mechs, E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4))
+    s.set_launch(kind=1, threads_per_cell=32, scratch_in_shared=1)
+    Yd = torch.as_tensor(Y, device="cuda")
+    md = torch.as_tensor(mid, device="cuda")
+    rho = torch.as_tensor(np.linspace(0.3, 1.1, n), device="cuda")
+
+    def direct(dT):
+        dtc = torch.full((n,), 1e-7, dtype=torch.float64, device="cuda")
+        out = s.solve(Yd, dT, dtc, rho=rho, mech_id=md)
+        torch.cuda.synchronize()
+        return (out["Ynew"].cpu().numpy(), out["RR"].cpu().numpy(), dtc.cpu().numpy(),
+                out["status"].cpu().numpy(), out["counters"].cpu().numpy(), out["stats"])
+
+    ref = direct(1e-5)
+    dtc = torch.empty(n, dtype=torch.float64, device="cuda")
+    status = torch.empty(n, dtype=torch.int32, device="cuda")
+    counters = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+    g = s.capture(Yd, 1e-5, dtc, rho=rho, mech_id=md, status=status, counters=counters)
+    stream = torch.cuda.Stream()
+    s.set_launch(kind=0)  # the graph keeps the launch form it was captured with
+    for _ in range(3):
+        dtc.fill_(1e-7)
+        g.launch(stream)
+        stream.synchronize()
+        got = (g["Ynew"].cpu().numpy(), g["RR"].cpu().numpy(), dtc.cpu().numpy(), status.cpu().numpy(),
+               counters.cpu().numpy())
+        for a, b in zip(got, ref[:5]):
+            assert np.array_equal(a, b)
+        assert g.stats() == ref[5]
+    s.set_launch(kind=1, threads_per_cell=32, scratch_in_shared=1)
+    ref2 = direct(3e-6)
+    g.set_delta_t(3e-6)
+    dtc.fill_(1e-7)
+    g.launch(stream)
+    stream.synchronize()
+    assert np.array_equal(g["Ynew"].cpu().numpy(), ref2[0])
+    assert np.array_equal(counters.cpu().numpy(), ref2[4])
+    assert g.stats() == ref2[5]
+    g.close()

@@ -44,7 +44,7 @@ def test_strerror(lib):
     assert lib.gf_strerror(2) == b"Invalid ODE Solver type"
 
 
-@pytest.mark.parametrize("name", ["h2size", "coverage", "grisize"])
+@pytest.mark.parametrize("name", ["h2size", "coverage", "grisize", "foam_h2", "foam_gri", "foam_yao"])
 def test_loader_arithmetic_matches_reference_tables(lib, name):
     from tests.test_oracle import fixture_mech
     g = dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))

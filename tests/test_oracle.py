@@ -19,7 +19,7 @@ from gpufoam_b200 import mechanism as M
 from oracle.oracle import REF_LIB, Oracle, lu, ode_inputs
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-CASES = ["h2size", "coverage", "grisize"]
+CASES = ["h2size", "coverage", "grisize", "foam_h2", "foam_gri", "foam_yao"]
 
 
 def load(name):
