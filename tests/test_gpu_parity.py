@@ -248,7 +248,8 @@ def test_graph_replay_matches_solve(torch):
 
     def direct(dT):
         dtc = torch.full((n,), 1e-7, dtype=torch.float64, device="cuda")
-        out = s.solve(Yd, dT, dtc, rho=rho, mech_id=md)
+        # zero-filled outputs: the columns past a cell's own nEqns / nSpecie are not written
+        out = s.solve(Yd, dT, dtc, rho=rho, mech_id=md, Ynew=torch.zeros_like(Yd), RR=torch.zeros_like(Yd))
         torch.cuda.synchronize()
         return (out["Ynew"].cpu().numpy(), out["RR"].cpu().numpy(), dtc.cpu().numpy(),
                 out["status"].cpu().numpy(), out["counters"].cpu().numpy(), out["stats"])
@@ -257,7 +258,8 @@ def test_graph_replay_matches_solve(torch):
     dtc = torch.empty(n, dtype=torch.float64, device="cuda")
     status = torch.empty(n, dtype=torch.int32, device="cuda")
     counters = torch.empty((n, 2), dtype=torch.int32, device="cuda")
-    g = s.capture(Yd, 1e-5, dtc, rho=rho, mech_id=md, status=status, counters=counters)
+    g = s.capture(Yd, 1e-5, dtc, rho=rho, mech_id=md, status=status, counters=counters,
+                  Ynew=torch.zeros_like(Yd), RR=torch.zeros_like(Yd))
     stream = torch.cuda.Stream()
     s.set_launch(kind=0)  # the graph keeps the launch form it was captured with
     for _ in range(3):
