@@ -30,7 +30,8 @@ EXPORTS = [
     "gf_compute_rr", "gf_compute_ynew", "gf_rates", "gf_jacobian", "gf_lu_decompose", "gf_lu_backsubstitute",
     "gf_strerror", "gf_abi_version", "gf_last_cuda_error", "gf_measure_fp64_peak", "gf_solve_noalloc",
     "gf_solve_record", "gf_adjoint", "gf_solve_graph_create", "gf_solve_graph_set_delta_t",
-    "gf_solve_graph_launch", "gf_solve_graph_stats", "gf_solve_graph_destroy",
+    "gf_solve_graph_launch", "gf_solve_graph_stats", "gf_solve_graph_destroy", "gf_cell_rates",
+    "gf_reaction_rates", "gf_qdot",
 ]
 
 
@@ -136,6 +137,9 @@ def load() -> C.CDLL:
     lib.gf_solve_graph_stats.argtypes = [vp, P(GfStats)]
     lib.gf_solve_graph_destroy.argtypes = [vp]
     lib.gf_solve_graph_destroy.restype = None
+    lib.gf_cell_rates.argtypes = [vp, ip, vp, vp, ip, vp, ip, vp, vp]
+    lib.gf_reaction_rates.argtypes = [vp, ip, ip, vp, vp, ip, vp, vp, ip, vp]
+    lib.gf_qdot.argtypes = [vp, ip, vp, ip, vp, vp]
     lib.gf_strerror.argtypes = [ip]
     lib.gf_strerror.restype = C.c_char_p
     lib.gf_abi_version.restype = ip

@@ -18,6 +18,7 @@ namespace {
 
 // gpu_utils/common/gpu_constants.H:13-82
 constexpr double kRR = 6.02214e+26 * 1.38065e-23;
+constexpr double kTstd = 298.15;  // gpu_constants.H
 constexpr double kSmall = DBL_EPSILON;
 constexpr double kVSmall = DBL_MIN;
 constexpr double kGreat = 1.0 / DBL_EPSILON;
@@ -147,6 +148,7 @@ std::vector<gf::StreamRec> build_stream(const std::vector<std::vector<std::pair<
 
 struct gf_mech {
     gf::DevMech dev;
+    std::vector<int> q_of_r;  // compute position of each reaction (mechanism order)
     void* dmem = nullptr;
     long long bytes = 0;
     int device = 0;
@@ -298,10 +300,14 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
         if (!(d->thermos[i].W > 0)) return GF_ERR_INVALID_ARGUMENT;
 
     // ---- host tables
-    std::vector<double> W(nS), Rsp(nS), Tc(nS), coef((size_t)14 * nS);
+    std::vector<double> W(nS), Rsp(nS), Tc(nS), coef((size_t)14 * nS), hf(nS);
     for (int i = 0; i < nS; ++i) {
         const gf_thermo& t = d->thermos[i];
         W[i] = t.W;
+        // enthalpy of formation, gpuThermo::Hf (gpuThermo.H:243-254), for Qdot
+        const double* a = t.low;
+        const double Ts = kTstd;
+        hf[i] = (((((a[4] / 5.0 * Ts + a[3] / 4.0) * Ts + a[2] / 3.0) * Ts + a[1] / 2.0) * Ts + a[0]) * Ts + a[5]);
         Rsp[i] = kRR / t.W;
         Tc[i] = t.Tcommon;
         for (int k = 0; k < 7; ++k) {
@@ -481,7 +487,7 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
 
     // ---- one device allocation
     DevBuf b;
-    const size_t oW = b.add(W), oR = b.add(Rsp), oTc = b.add(Tc), oCoef = b.add(coef);
+    const size_t oW = b.add(W), oR = b.add(Rsp), oTc = b.add(Tc), oCoef = b.add(coef), oHf = b.add(hf);
     const size_t oRt = b.add(rtype), oRi = b.add(rirr), oNl = b.add(nl), oNr = b.add(nr), oSpo = b.add(sp_off),
                  oSlot = b.add(slot), oRY = b.add(rY), oRnm = b.add(rnm), oRns = b.add(rnm_small), oRTc = b.add(rTc),
                  oRc = b.add(rcoef), oLA0 = b.add(lnA0), oSA0 = b.add(sA0), oB0 = b.add(beta0), oT0 = b.add(Ta0),
@@ -523,6 +529,7 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     D.Rsp = (const double*)P(oR);
     D.Tcommon = (const double*)P(oTc);
     D.coef = (const double*)P(oCoef);
+    D.hf = (const double*)P(oHf);
     D.rtype = (const int*)P(oRt);
     D.rirr = (const int*)P(oRi);
     D.nl = (const int*)P(oNl);
@@ -558,6 +565,7 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
         D.cst[k] = Stream{(const StreamRec*)P(oCst[k]), cst_len[k]};
     }
     D.max_side = max_side;
+    m->q_of_r.assign(rof.begin(), rof.begin() + nR);
     *out = m;
     return GF_OK;
 }
@@ -879,6 +887,35 @@ void gf_solve_graph_destroy(gf_solve_graph* g) {
     cudaFree(g->queue);
     if (g->queue_host) cudaFreeHost(g->queue_host);
     delete g;
+}
+
+// ---- the plugin's per-cell side paths (gf_fields.cu) --------------------------
+
+int gf_cell_rates(const gf_mech* m, int n_cells, const double* rho, const double* y, int ld_y, double* RR,
+                  int ld_rr, double* tc, void* stream) {
+    if (!m || n_cells < 0 || (n_cells > 0 && (!rho || !y))) return GF_ERR_INVALID_ARGUMENT;
+    if (ld_y < m->dev.nS + 2 || (RR && ld_rr < m->dev.nS)) return GF_ERR_INVALID_ARGUMENT;
+    if (!RR && !tc) return GF_OK;
+    gf::FieldArgs a{n_cells, rho, y, ld_y, RR, ld_rr, tc, -1, -1, nullptr};
+    const int e = gf::launch_cell_fields(m->dev, a, stream);
+    return e ? (e == (int)cudaErrorInvalidValue ? GF_ERR_UNSUPPORTED : cuda_fail((cudaError_t)e)) : GF_OK;
+}
+
+int gf_reaction_rates(const gf_mech* m, int n_cells, int reaction, const double* rho, const double* y, int ld_y,
+                      double* omega, double* RR, int ld_rr, void* stream) {
+    if (!m || n_cells < 0 || (n_cells > 0 && (!rho || !y))) return GF_ERR_INVALID_ARGUMENT;
+    if (reaction < 0 || reaction >= m->dev.nR) return GF_ERR_INVALID_ARGUMENT;
+    if (ld_y < m->dev.nS + 2 || (RR && ld_rr < m->dev.nS)) return GF_ERR_INVALID_ARGUMENT;
+    if (!RR && !omega) return GF_OK;
+    gf::FieldArgs a{n_cells, rho, y, ld_y, RR, ld_rr, nullptr, reaction, m->q_of_r[reaction], omega};
+    const int e = gf::launch_cell_fields(m->dev, a, stream);
+    return e ? (e == (int)cudaErrorInvalidValue ? GF_ERR_UNSUPPORTED : cuda_fail((cudaError_t)e)) : GF_OK;
+}
+
+int gf_qdot(const gf_mech* m, int n_cells, const double* RR, int ld_rr, double* qdot, void* stream) {
+    if (!m || n_cells < 0 || (n_cells > 0 && (!RR || !qdot)) || ld_rr < m->dev.nS) return GF_ERR_INVALID_ARGUMENT;
+    const int e = gf::launch_qdot(m->dev, n_cells, RR, ld_rr, qdot, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
 }
 
 // gf_solve with the trajectory recorded for the adjoint (single mechanism).

@@ -81,6 +81,7 @@ struct DevMech {
     const double* Rsp;         // RR / W
     const double* Tcommon;
     const double* coef;
+    const double* hf;          // enthalpy of formation [J/kg] (Qdot)
     // reactions, compute order
     const int* rtype;
     const int* rirr;
@@ -184,6 +185,22 @@ int launch_adjoint_cells(const DevMech& m, int n_cells, const double* traj, int 
                          long long ws_per_cell, int n_blocks, unsigned long long* queue, void* stream);
 int adjoint_blocks_per_sm(const DevMech& m);
 int launch_record(const DevMech& m, const LaunchArgs& a, void* stream);
+
+// The plugin's per-cell side paths (gf_fields.cu).
+struct FieldArgs {
+    int n_cells;
+    const double* rho;
+    const double* y;
+    int ld_y;
+    double* RR;        // calculate() / specieReactionRR(r) [n][ld_rr] or null
+    int ld_rr;
+    double* tc;        // tc() [n] or null
+    int reaction;      // >= 0: reactionRR / specieReactionRR of this reaction
+    int reaction_q;    // its compute position
+    double* omega;     // reactionRR(r) [n] or null
+};
+int launch_cell_fields(const DevMech& m, const FieldArgs& a, void* stream);
+int launch_qdot(const DevMech& m, int n_cells, const double* RR, int ld_rr, double* qdot, void* stream);
 
 // Device tables of a mechanism object (gf_host.cpp).
 const DevMech* mech_device_tables(const gf_mech* m);

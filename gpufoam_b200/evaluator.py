@@ -401,3 +401,40 @@ def lu_backsubstitute(LU, piv, b):
     N.check(lib.gf_lu_backsubstitute(k, m, _ptr(_dev(LU, torch.float64)), _ptr(_dev(piv, torch.int32)), _ptr(bd),
                                      _stream_ptr()), "gf_lu_backsubstitute")
     return bd
+
+
+# ---- the plugin's per-cell side paths (gpuChemistryModel.C:145-450), on the GPU
+
+def cell_rates(mech: Mechanism, rho, y, want_RR: bool = True, want_tc: bool = True):
+    """calculate() and tc() at c = rho Y / W: (RR [n][nS] or None, tc [n] or None), cuda tensors."""
+    import torch
+    yd = _dev(y, torch.float64)
+    rd = _dev(rho, torch.float64)
+    n = yd.shape[0]
+    RR = torch.empty((n, mech.n_species), dtype=torch.float64, device="cuda") if want_RR else None
+    tc = torch.empty(n, dtype=torch.float64, device="cuda") if want_tc else None
+    N.check(mech.lib.gf_cell_rates(mech.handle, n, _ptr(rd), _ptr(yd), yd.shape[1], _ptr(RR), mech.n_species,
+                                   _ptr(tc), _stream_ptr()), "gf_cell_rates")
+    return RR, tc
+
+
+def reaction_rates(mech: Mechanism, reaction: int, rho, y):
+    """reactionRR(r) and specieReactionRR(r): (omega [n], RR [n][nS]), cuda tensors."""
+    import torch
+    yd = _dev(y, torch.float64)
+    rd = _dev(rho, torch.float64)
+    n = yd.shape[0]
+    om = torch.empty(n, dtype=torch.float64, device="cuda")
+    RR = torch.empty((n, mech.n_species), dtype=torch.float64, device="cuda")
+    N.check(mech.lib.gf_reaction_rates(mech.handle, n, int(reaction), _ptr(rd), _ptr(yd), yd.shape[1], _ptr(om),
+                                       _ptr(RR), mech.n_species, _stream_ptr()), "gf_reaction_rates")
+    return om, RR
+
+
+def qdot(mech: Mechanism, RR):
+    """Qdot() from species mass rates RR [n][nS] (host or device) -> cuda tensor [n]."""
+    import torch
+    rd = _dev(RR, torch.float64)
+    out = torch.empty(rd.shape[0], dtype=torch.float64, device="cuda")
+    N.check(mech.lib.gf_qdot(mech.handle, rd.shape[0], _ptr(rd), rd.shape[1], _ptr(out), _stream_ptr()), "gf_qdot")
+    return out

@@ -247,6 +247,31 @@ int gf_compute_ynew(gf_solver* solver, int n_cells, double deltaT, double deltaT
                     const double* deltaTChem, const double* Y, double* Ynew,
                     double* deltaTChemNew);
 
+/* ---- the plugin's per-cell side paths ------------------------------------
+ * gpuChemistryModel computes these on the CPU through OpenFOAM's reactions
+ * (gpu_chemistry/src/gpuChemistryModels/gpuChemistryModel/gpuChemistryModel.C);
+ * here they run on the GPU with the solve's rate code. Concentrations are
+ * c_i = rho Y_i / W_i with the thermo's density rho [n_cells] (:163-166);
+ * y [n_cells][ld_y] = (Y, T, p); device pointers. */
+
+/*   gf_cell_rates       calculate()   gpuChemistryModel.C:145-186  RR [n][ld_rr] = W_i dN_i/dt / V
+ *                       tc()          gpuChemistryModel.C:366-427  tc [n], the chemical time scale
+ * Either output may be NULL. GF_ERR_UNSUPPORTED if one cell's rate data
+ * (about (2 nS + n_third_body + 4 nR) doubles) exceeds the shared memory of a CTA. */
+int gf_cell_rates(const gf_mech* mech, int n_cells, const double* rho, const double* y, int ld_y,
+                  double* RR, int ld_rr, double* tc, void* stream);
+
+/*   gf_reaction_rates   reactionRR(r)        gpuChemistryModel.C:188-229  omega [n] of reaction r
+ *                       specieReactionRR(r)  gpuChemistryModel.C:231-298  RR [n][ld_rr] of reaction r alone
+ * reaction in mechanism order; either output may be NULL. */
+int gf_reaction_rates(const gf_mech* mech, int n_cells, int reaction, const double* rho, const double* y,
+                      int ld_y, double* omega, double* RR, int ld_rr, void* stream);
+
+/*   gf_qdot             Qdot()        gpuChemistryModel.C:429-450  qdot [n] = -sum_i hf_i RR[c][i]
+ * from species mass rates RR (of gf_solve, gf_compute_rr or gf_cell_rates),
+ * hf_i the enthalpy of formation (gpuThermo::Hf); summed in species order. */
+int gf_qdot(const gf_mech* mech, int n_cells, const double* RR, int ld_rr, double* qdot, void* stream);
+
 /* ---- differentiation (no counterpart in the reference) ------------------ */
 
 /* gf_solve (single mechanism, one flow step deltaT, no RR) that also records

@@ -1056,6 +1056,119 @@ double orc_compute_rr_host(int nc, int nS, double deltaT, double deltaTChemMax, 
     return mn;
 }
 
+/* ---- the plugin's per-cell side paths (gpuChemistryModel.C), on the
+ * concentrations c_i = rho Y_i / W_i of the thermo's density ---- */
+
+static void field_c(const mech_t* m, double rho, const double* y, double* c) {
+    for (int i = 0; i < m->nS; ++i) c[i] = rho * y[i] / m->th[i].W; /* :163-166 */
+}
+
+/* calculate() :145-186 (RR [n][nS]) and tc() :366-427 ([n]); either may be NULL */
+void orc_cell_fields(void* h, int nc, const double* rho, const double* y, double* RR, double* tc) {
+    const mech_t* m = (const mech_t*)h;
+    const int nS = m->nS, ne = nS + 2;
+    double* c = (double*)malloc(sizeof(double) * (nS > 0 ? nS : 1));
+    double* dN = (double*)malloc(sizeof(double) * (nS > 0 ? nS : 1));
+    for (int j = 0; j < nc; ++j) {
+        const double* yj = y + (size_t)j * ne;
+        const double T = yj[nS], p = yj[nS + 1];
+        field_c(m, rho[j], yj, c);
+        if (RR) {
+            for (int i = 0; i < nS; ++i) dN[i] = 0.0;
+            for (int r = 0; r < m->nR; ++r) { /* gpuReaction.H:490-508 */
+                const rxn_t* R = &m->rx[r];
+                const double om = rxn_omega(R, nS, p, T, c);
+                for (int k = 0; k < R->nl; ++k) dN[R->lhs[k].index] -= R->lhs[k].stoich * om;
+                for (int k = 0; k < R->nr; ++k) dN[R->rhs[k].index] += R->rhs[k].stoich * om;
+            }
+            for (int i = 0; i < nS; ++i) RR[(size_t)j * nS + i] = dN[i] * m->th[i].W;
+        }
+        if (tc) {
+            double sumW = 0, sumWRateByCTot = 0;
+            for (int r = 0; r < m->nR; ++r) {
+                const rxn_t* R = &m->rx[r];
+                const double clippedT = fmin(fmax(T, R->Tlow), R->Thigh);
+                const double kf = rate_k(R, nS, clippedT, c);
+                const double kr = R->irr ? 0.0 : kf / th_Kc(&R->th, clippedT);
+                double Cf = 1.0, Cr = 1.0;
+                for (int k = 0; k < R->nl; ++k) Cf *= specie_pow(c[R->lhs[k].index], &R->lhs[k]);
+                for (int k = 0; k < R->nr; ++k) Cr *= specie_pow(c[R->rhs[k].index], &R->rhs[k]);
+                const double omegaf = kf * Cf, omegar = kr * Cr;
+                double wf = 0;
+                for (int k = 0; k < R->nr; ++k) wf += R->rhs[k].stoich * omegaf;
+                sumW += wf;
+                sumWRateByCTot += wf * wf;
+                double wr = 0;
+                for (int k = 0; k < R->nl; ++k) wr += R->lhs[k].stoich * omegar;
+                sumW += wr;
+                sumWRateByCTot += wr * wr;
+            }
+            double ctot = 0;
+            for (int i = 0; i < nS; ++i) ctot += c[i];
+            tc[j] = sumWRateByCTot == 0 ? ORC_VGREAT : sumW / sumWRateByCTot * ctot;
+        }
+    }
+    free(c);
+    free(dN);
+}
+
+/* Test helper: (kf Cf, kr Cr) of every reaction [n][nR][2] at c = rho Y / W,
+ * the gross forward and reverse rates that bound the rounding of the net ones. */
+void orc_rate_parts(void* h, int nc, const double* rho, const double* y, double* out) {
+    const mech_t* m = (const mech_t*)h;
+    const int nS = m->nS, ne = nS + 2;
+    double* c = (double*)malloc(sizeof(double) * (nS > 0 ? nS : 1));
+    for (int j = 0; j < nc; ++j) {
+        const double* yj = y + (size_t)j * ne;
+        const double T = yj[nS];
+        field_c(m, rho[j], yj, c);
+        for (int r = 0; r < m->nR; ++r) {
+            const rxn_t* R = &m->rx[r];
+            const double clippedT = fmin(fmax(T, R->Tlow), R->Thigh);
+            const double kf = rate_k(R, nS, clippedT, c);
+            const double kr = R->irr ? 0.0 : kf / th_Kc(&R->th, clippedT);
+            double Cf = 1.0, Cr = 1.0;
+            for (int k = 0; k < R->nl; ++k) Cf *= specie_pow(c[R->lhs[k].index], &R->lhs[k]);
+            for (int k = 0; k < R->nr; ++k) Cr *= specie_pow(c[R->rhs[k].index], &R->rhs[k]);
+            out[((size_t)j * m->nR + r) * 2] = kf * Cf;
+            out[((size_t)j * m->nR + r) * 2 + 1] = kr * Cr;
+        }
+    }
+    free(c);
+}
+
+/* reactionRR(r) :188-229 (omega [n]) and specieReactionRR(r) :231-298 (RR [n][nS]) */
+void orc_reaction_fields(void* h, int nc, int r, const double* rho, const double* y, double* omega, double* RR) {
+    const mech_t* m = (const mech_t*)h;
+    const int nS = m->nS, ne = nS + 2;
+    const rxn_t* R = &m->rx[r];
+    double* c = (double*)malloc(sizeof(double) * (nS > 0 ? nS : 1));
+    for (int j = 0; j < nc; ++j) {
+        const double* yj = y + (size_t)j * ne;
+        field_c(m, rho[j], yj, c);
+        const double om = rxn_omega(R, nS, yj[nS + 1], yj[nS], c);
+        if (omega) omega[j] = om;
+        if (RR) {
+            double* o = RR + (size_t)j * nS;
+            for (int i = 0; i < nS; ++i) o[i] = 0.0;
+            for (int k = 0; k < R->nl; ++k) o[R->lhs[k].index] -= R->lhs[k].stoich * om;
+            for (int k = 0; k < R->nr; ++k) o[R->rhs[k].index] += R->rhs[k].stoich * om;
+            for (int i = 0; i < nS; ++i) o[i] = o[i] * m->th[i].W;
+        }
+    }
+    free(c);
+}
+
+/* Qdot() :429-450: Qdot = 0 - sum_i hf_i RR_i in species order */
+void orc_qdot(void* h, int nc, const double* RR, double* qdot) {
+    const mech_t* m = (const mech_t*)h;
+    for (int j = 0; j < nc; ++j) {
+        double q = 0;
+        for (int i = 0; i < m->nS; ++i) q -= th_Hf(&m->th[i]) * RR[(size_t)j * m->nS + i];
+        qdot[j] = q;
+    }
+}
+
 void orc_constants(double* out) {
     out[0] = ORC_RR;
     out[1] = ORC_PSTD;

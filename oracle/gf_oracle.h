@@ -54,6 +54,11 @@ void orc_cells(void* h, const orc_ode_inputs* o, double Treact, int n, double de
 double orc_compute_rr_host(int n, int nS, double deltaT, double deltaTChemMax, const double* rho,
                            const double* Y0, const double* Ynew, double* deltaTChemNew, double* RR);
 void orc_constants(double* out);
+void orc_cell_fields(void* h, int n, const double* rho, const double* y, double* RR, double* tc);
+void orc_reaction_fields(void* h, int n, int reaction, const double* rho, const double* y, double* omega,
+                         double* RR);
+void orc_qdot(void* h, int n, const double* RR, double* qdot);
+void orc_rate_parts(void* h, int n, const double* rho, const double* y, double* out);
 
 #ifdef __cplusplus
 }

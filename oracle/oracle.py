@@ -119,6 +119,12 @@ class Oracle:
         f.restype = C.c_double
         f.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]
         getattr(L, p + "constants").argtypes = [_dp]
+        getattr(L, p + "cell_fields").argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_void_p, C.c_void_p]
+        getattr(L, p + "reaction_fields").argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, C.c_void_p,
+                                                      C.c_void_p]
+        getattr(L, p + "qdot").argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        if kind == "port":
+            L.orc_rate_parts.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
         self.mech = mech
         fl = flatten(mech)
         self._flat = fl
@@ -219,6 +225,42 @@ class Oracle:
             n, self.nS, deltaT, deltaTChemMax, np.ascontiguousarray(rho, dtype=np.float64),
             np.ascontiguousarray(Y0), np.ascontiguousarray(Ynew), dtc, RR)
         return RR, dtc, mn
+
+    # ---- the plugin's per-cell side paths (gpuChemistryModel.C:145-450)
+    def cell_fields(self, rho, y):
+        """calculate() and tc(): (RR [n][nS], tc [n]) at c = rho Y / W."""
+        y = np.ascontiguousarray(np.atleast_2d(y), dtype=np.float64)
+        n = y.shape[0]
+        RR = np.zeros((n, self.nS))
+        tc = np.zeros(n)
+        getattr(self.lib, self._p + "cell_fields")(self.h, n, np.ascontiguousarray(rho, dtype=np.float64), y,
+                                                   RR.ctypes.data_as(C.c_void_p), tc.ctypes.data_as(C.c_void_p))
+        return RR, tc
+
+    def reaction_fields(self, reaction, rho, y):
+        """reactionRR(r) and specieReactionRR(r): (omega [n], RR [n][nS])."""
+        y = np.ascontiguousarray(np.atleast_2d(y), dtype=np.float64)
+        n = y.shape[0]
+        om = np.zeros(n)
+        RR = np.zeros((n, self.nS))
+        getattr(self.lib, self._p + "reaction_fields")(self.h, n, int(reaction),
+                                                       np.ascontiguousarray(rho, dtype=np.float64), y,
+                                                       om.ctypes.data_as(C.c_void_p), RR.ctypes.data_as(C.c_void_p))
+        return om, RR
+
+    def rate_parts(self, rho, y):
+        """(kf Cf, kr Cr) [n][nR][2] at c = rho Y / W (port only; tolerance scales)."""
+        y = np.ascontiguousarray(np.atleast_2d(y), dtype=np.float64)
+        out = np.zeros((y.shape[0], max(self.nR, 1), 2))
+        self.lib.orc_rate_parts(self.h, y.shape[0], np.ascontiguousarray(rho, dtype=np.float64), y, out)
+        return out[:, : self.nR]
+
+    def qdot(self, RR):
+        """Qdot() from species mass rates RR [n][nS]."""
+        RR = np.ascontiguousarray(np.atleast_2d(RR), dtype=np.float64)
+        out = np.zeros(RR.shape[0])
+        getattr(self.lib, self._p + "qdot")(self.h, RR.shape[0], RR, out)
+        return out
 
     def constants(self):
         out = np.zeros(9)

@@ -399,6 +399,81 @@ double ref_compute_rr_host(int n, int nS, double deltaT, double deltaTChemMax, c
     return mn;
 }
 
+// The plugin's per-cell side paths (gpuChemistryModel.C) on the reference's
+// own reactions: c_i = rho Y_i / W_i (:163-166); calculate() :145-186 (RR,
+// dNdtByV in mechanism order times W), tc() :366-427 with omegaf = kf Cf and
+// omegar = kr Cr split as gpuReaction::omega computes them (gpuReaction.H:472-488).
+void ref_cell_fields(void* h, int n, const double* rho, const double* y, double* RR, double* tc) {
+    auto* m = static_cast<RefMech*>(h);
+    const int nS = m->nS, ne = nS + 2;
+    std::vector<double> c(nS), dN(nS);
+    auto cc = mdspan<const gScalar, 1>(c.data(), extents<1>{nS});
+    for (int j = 0; j < n; ++j) {
+        const double* yj = y + (size_t)j * ne;
+        const double T = yj[nS], p = yj[nS + 1];
+        for (int i = 0; i < nS; ++i) c[i] = rho[j] * yj[i] / m->thermos[i].W();
+        if (RR) {
+            std::fill(dN.begin(), dN.end(), 0.0);
+            auto ds = mdspan<gScalar, 1>(dN.data(), extents<1>{nS});
+            for (int r = 0; r < m->nR; ++r) m->reactions[r].dNdtByV(p, T, cc, ds);
+            for (int i = 0; i < nS; ++i) RR[(size_t)j * nS + i] = dN[i] * m->thermos[i].W();
+        }
+        if (tc) {
+            double sumW = 0, sumWRateByCTot = 0;
+            for (int r = 0; r < m->nR; ++r) {
+                const gpuReaction& R = m->reactions[r];
+                const gScalar clippedT = fmin(fmax(T, R.Tlow()), R.Thigh());
+                const gScalar kf = R.kf(p, clippedT, cc);
+                const gScalar kr = R.kr(kf, p, clippedT, R.Kc(p, clippedT), cc);
+                const gScalar omegaf = kf * R.calcCf(R.lhsPowers(cc));
+                const gScalar omegar = kr * R.calcCr(R.rhsPowers(cc));
+                double wf = 0;
+                for (size_t s = 0; s < R.rhs().size(); ++s) wf += R.rhs()[s].stoichCoeff * omegaf;
+                sumW += wf;
+                sumWRateByCTot += wf * wf;
+                double wr = 0;
+                for (size_t s = 0; s < R.lhs().size(); ++s) wr += R.lhs()[s].stoichCoeff * omegar;
+                sumW += wr;
+                sumWRateByCTot += wr * wr;
+            }
+            double ctot = 0;
+            for (int i = 0; i < nS; ++i) ctot += c[i];
+            tc[j] = sumWRateByCTot == 0 ? gpuVGreat : sumW / sumWRateByCTot * ctot;
+        }
+    }
+}
+
+// reactionRR(r) :188-229 and specieReactionRR(r) :231-298.
+void ref_reaction_fields(void* h, int n, int r, const double* rho, const double* y, double* omega, double* RR) {
+    auto* m = static_cast<RefMech*>(h);
+    const int nS = m->nS, ne = nS + 2;
+    const gpuReaction& R = m->reactions[r];
+    std::vector<double> c(nS);
+    auto cc = mdspan<const gScalar, 1>(c.data(), extents<1>{nS});
+    for (int j = 0; j < n; ++j) {
+        const double* yj = y + (size_t)j * ne;
+        for (int i = 0; i < nS; ++i) c[i] = rho[j] * yj[i] / m->thermos[i].W();
+        const double om = R.omega(yj[nS + 1], yj[nS], cc);
+        if (omega) omega[j] = om;
+        if (RR) {
+            double* o = RR + (size_t)j * nS;
+            std::fill(o, o + nS, 0.0);
+            R.dNdtByV(om, mdspan<gScalar, 1>(o, extents<1>{nS}));
+            for (int i = 0; i < nS; ++i) o[i] = o[i] * m->thermos[i].W();
+        }
+    }
+}
+
+// Qdot() :429-450 with gpuThermo::Hf (gpuThermo.H:243-254) for hf.
+void ref_qdot(void* h, int n, const double* RR, double* qdot) {
+    auto* m = static_cast<RefMech*>(h);
+    for (int j = 0; j < n; ++j) {
+        double q = 0;
+        for (int i = 0; i < m->nS; ++i) q -= m->thermos[i].Hf() * RR[(size_t)j * m->nS + i];
+        qdot[j] = q;
+    }
+}
+
 // Reference constants (gpu_constants.H): RR, pStd, Tstd, NNA, k, vGreat, vSmall, small, great
 void ref_constants(double* out) {
     out[0] = gpuRR;
