@@ -36,14 +36,14 @@ constexpr int kMaxRejects = 100000;  // rejected attempts within one substep
 // lane 0 of each group accumulates clock64() cycles per phase of the solve.
 #ifdef GF_PHASE_TIMERS
 // one accumulator per translation unit (each has its own device module)
-static __device__ unsigned long long g_phase_cycles[16];
-// adds this translation unit's accumulators to out[16], optionally clearing them
+static __device__ unsigned long long g_phase_cycles[20];
+// adds this translation unit's accumulators to out[20], optionally clearing them
 static inline int phase_cycles_local(unsigned long long* out, int reset) {
-    unsigned long long v[16];
+    unsigned long long v[20];
     cudaMemcpyFromSymbol(v, g_phase_cycles, sizeof(v));
-    for (int i = 0; i < 16; ++i) out[i] += v[i];
+    for (int i = 0; i < 20; ++i) out[i] += v[i];
     if (reset) {
-        unsigned long long z[16] = {};
+        unsigned long long z[20] = {};
         cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
     }
     return (int)cudaGetLastError();
@@ -59,7 +59,8 @@ static inline int phase_cycles_local(unsigned long long* out, int reset) {
 #define GF_PH_END(g, k)
 #endif
 enum { PH_MIX = 0, PH_NMPOW, PH_OMEGA, PH_GATHER_RHS, PH_JPARAMS, PH_JROWS, PH_TROW, PH_SHIFT, PH_LU, PH_SOLVE,
-       PH_ADJ_RXN, PH_ATTEMPT, PH_ADJ_RECOMPUTE, PH_ADJ_TSOLVE, PH_ADJ_VJP, PH_ADJ_JTERM };
+       PH_ADJ_RXN, PH_ATTEMPT, PH_ADJ_RECOMPUTE, PH_ADJ_TSOLVE, PH_ADJ_VJP, PH_ADJ_JTERM, PH_LU_PANEL, PH_LU_U12,
+       PH_LU_TRAIL };
 
 // ---------------------------------------------------------------- groups
 
@@ -342,13 +343,17 @@ __device__ __forceinline__ double integer_pow(double x, int e) {
     }
     return y;
 }
+// x^e for a non-integer exponent (rare: most mechanisms have integer
+// exponents only), out of line: the many call sites share one copy of the
+// math library's pow, which keeps the solve's instruction footprint smaller.
+static __device__ __noinline__ double real_pow(double x, double e) { return pow(x, e); }
 // gpuSpecieExponent.H:103-110
 __device__ __forceinline__ double specie_pow(double x, int iexp, double sexp) {
-    return iexp != kNoIntExp ? integer_pow(x, iexp) : pow(x, sexp);
+    return iexp != kNoIntExp ? integer_pow(x, iexp) : real_pow(x, sexp);
 }
 // speciePow(c, e - 1) (gpuReaction.H:418-420 with gpuSpecieExponent::operator-)
 __device__ __forceinline__ double specie_pow_m1(double x, int iexp, double sexp) {
-    return iexp != kNoIntExp ? integer_pow(x, iexp - 1) : pow(x, sexp + (-1.0));
+    return iexp != kNoIntExp ? integer_pow(x, iexp - 1) : real_pow(x, sexp + (-1.0));
 }
 
 // ln|k| of an Arrhenius factor: k (or the fall-off k0) from the reaction's
@@ -1162,46 +1167,58 @@ __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& 
     for (int k0 = 0; k0 < m; ) {
         const int kb = min(NB, m - k0);
         const int k1 = k0 + kb;
-        if (wid == 0) {
-            Grp<32> g32;
-            lu_panel_reg<2, NB>(g32, w, A, ld, piv, vv, m, k0, k1);
+        {
+            GF_PH_BEGIN(g)
+            if (wid == 0) {
+                Grp<32> g32;
+                lu_panel_reg<2, NB>(g32, w, A, ld, piv, vv, m, k0, k1);
+            }
+            g.sync();
+            GF_PH_END(g, PH_LU_PANEL)
         }
-        g.sync();
-        // row exchanges outside the panel, and U12 of the columns right of it
-        for (int j = g.lane; j < m - kb; j += G) {
-            const int jj = j < k0 ? j : j + kb;
-            lu_apply_swaps(w, A, ld, piv, k0, k1, jj);
-            if (jj >= k1) {
-                double u[NB];
+        {
+            GF_PH_BEGIN(g)
+            // row exchanges outside the panel, and U12 of the columns right of it
+            for (int j = g.lane; j < m - kb; j += G) {
+                const int jj = j < k0 ? j : j + kb;
+                lu_apply_swaps(w, A, ld, piv, k0, k1, jj);
+                if (jj >= k1) {
+                    double u[NB];
 #pragma unroll
-                for (int t = 0; t < NB; ++t) u[t] = t < kb ? w[A + (k0 + t) * ld + jj] : 0.0;
+                    for (int t = 0; t < NB; ++t) u[t] = t < kb ? w[A + (k0 + t) * ld + jj] : 0.0;
 #pragma unroll
-                for (int t = 1; t < NB; ++t) {
-                    if (t < kb) {
-                        double v = u[t];
+                    for (int t = 1; t < NB; ++t) {
+                        if (t < kb) {
+                            double v = u[t];
 #pragma unroll
-                        for (int t2 = 0; t2 < t; ++t2) v -= w[A + (k0 + t) * ld + k0 + t2] * u[t2];
-                        u[t] = v;
-                        w[A + (k0 + t) * ld + jj] = v;
+                            for (int t2 = 0; t2 < t; ++t2) v -= w[A + (k0 + t) * ld + k0 + t2] * u[t2];
+                            u[t] = v;
+                            w[A + (k0 + t) * ld + jj] = v;
+                        }
                     }
                 }
             }
+            g.sync();
+            GF_PH_END(g, PH_LU_U12)
         }
-        g.sync();
         if (k1 >= m) break;
-        for (int j = k1 + l; j < m; j += 32) {
-            double u[NB];
+        {
+            GF_PH_BEGIN(g)
+            for (int j = k1 + l; j < m; j += 32) {
+                double u[NB];
 #pragma unroll
-            for (int t = 0; t < NB; ++t) u[t] = t < kb ? w[A + (k0 + t) * ld + j] : 0.0;
-            for (int i = k1 + wid; i < m; i += NWp) {
-                double a = w[A + i * ld + j];
+                for (int t = 0; t < NB; ++t) u[t] = t < kb ? w[A + (k0 + t) * ld + j] : 0.0;
+                for (int i = k1 + wid; i < m; i += NWp) {
+                    double a = w[A + i * ld + j];
 #pragma unroll
-                for (int t = 0; t < NB; ++t)
-                    if (t < kb) a -= w[A + i * ld + k0 + t] * u[t];
-                w[A + i * ld + j] = a;
+                    for (int t = 0; t < NB; ++t)
+                        if (t < kb) a -= w[A + i * ld + k0 + t] * u[t];
+                    w[A + i * ld + j] = a;
+                }
             }
+            g.sync();
+            GF_PH_END(g, PH_LU_TRAIL)
         }
-        g.sync();
         k0 = k1;
     }
 }
@@ -1561,40 +1578,20 @@ __device__ __forceinline__ double ros_d(const RosCoeffs& C, int i) {
 template <int G, class W, bool SAVE = false>
 __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
                               const OdeParams& o, int y0_off, int yt_off, double p, double dx, int save_y2 = -1,
-                              int save_y3 = -1) {
+                              int save_y3 = -1, bool first_deriv = false) {
     const int m = M.m;
     const int ld = L.ld;
-    jacobian(g, M, w, L, y0_off, p, true);
-    {
-        GF_PH_BEGIN(g)
-        shift_and_scale(g, w, L.J, ld, L.vv, m, 1.0 / (C.gamma * dx));
-        GF_PH_END(g, PH_SHIFT)
-    }
-    {
-        GF_PH_BEGIN(g)
-        bool done = false;
-        if constexpr (G >= 32) {
-            if (m <= 64) {
-                lu_decompose_regpanel<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
-                done = true;
-            }
-        }
-        if (!done) lu_decompose_blocked<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
-        GF_PH_END(g, PH_LU)
-    }
-    if (G >= 16) {
-        // the row scaling vv is no longer needed: it holds 1 / U[i][i] from here
-        for (int i = g.lane; i < m; i += G) w[L.vv + i] = 1.0 / w[L.J + i * ld + i];
-        lu_perm(g, w, L.piv, L.perm, m);
-    }
     // stages: k_i solves (I/(gamma dx) - J) k_i = f_i + dx d_i dfdx + sum_j c_ij k_j / dx,
     // f_0 = f(y0), f_i = f(y0 + sum_j a_ij k_j) where the method takes a new
     // derivative (stage 1; stage 2 of Rosenbrock34), else the previous one.
-    // One loop, so the solve and the derivative each have a single call site.
+    // One loop, so the solve and the derivative each have a single call site:
+    // pass st = -1 evaluates the step's f(y0) (first_deriv: the first attempt
+    // of a step) and then the Jacobian and its LU.
 #pragma unroll 1
-    for (int st = 0; st < C.s; ++st) {
-        const int ki = L.k1 + st * m;
-        if (st == 1 || (st == 2 && C.s == 4)) {
+    for (int st = -1; st < C.s; ++st) {
+        const bool new_f = st < 0 ? first_deriv : (st == 1 || (st == 2 && C.s == 4));
+        int at = y0_off, out = L.dydx0;
+        if (st > 0 && new_f) {
             // the stage point (kept at save_y2 / save_y3 when asked: the adjoint sweep)
             const int pt = !SAVE ? yt_off : (st == 1 ? save_y2 : (st == 2 ? save_y3 : yt_off));
             for (int i = g.lane; i < m; i += G) {
@@ -1602,8 +1599,37 @@ __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M,
                 for (int j = 0; j < st; ++j) v += ros_a(C, st, j) * w[L.k1 + j * m + i];
                 w[pt + i] = v;
             }
-            derivatives(g, M, w, L, pt, p, L.dydx);
+            at = pt;
+            out = L.dydx;
         }
+        if (new_f) derivatives(g, M, w, L, at, p, out, st < 0);
+        if (st < 0) {
+            jacobian(g, M, w, L, y0_off, p, true);
+            {
+                GF_PH_BEGIN(g)
+                shift_and_scale(g, w, L.J, ld, L.vv, m, 1.0 / (C.gamma * dx));
+                GF_PH_END(g, PH_SHIFT)
+            }
+            {
+                GF_PH_BEGIN(g)
+                bool done = false;
+                if constexpr (G >= 32) {
+                    if (m <= 64) {
+                        lu_decompose_regpanel<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
+                        done = true;
+                    }
+                }
+                if (!done) lu_decompose_blocked<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
+                GF_PH_END(g, PH_LU)
+            }
+            if (G >= 16) {
+                // the row scaling vv is no longer needed: it holds 1 / U[i][i] from here
+                for (int i = g.lane; i < m; i += G) w[L.vv + i] = 1.0 / w[L.J + i * ld + i];
+                lu_perm(g, w, L.piv, L.perm, m);
+            }
+            continue;
+        }
+        const int ki = L.k1 + st * m;
         const int src = st == 0 ? L.dydx0 : L.dydx;
         const double dd = dx * ros_d(C, st);
         for (int i = g.lane; i < m; i += G) {
@@ -1673,10 +1699,11 @@ __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, cons
         double dx = step_dxTry;
         double err = 0.0;
         int rejects = 0;
-        derivatives(g, M, w, L, *y_off, p, L.dydx0, true);
         do {
             GF_PH_BEGIN(g)
-            err = ros_attempt(g, M, w, L, C, o, *y_off, *yt_off, p, dx);
+            // the first attempt of the step also evaluates f(y0) (adaptiveSolve's
+            // derivatives call before its retry loop, gpuAdaptiveSolver.H:96)
+            err = ros_attempt(g, M, w, L, C, o, *y_off, *yt_off, p, dx, -1, -1, rejects == 0);
             GF_PH_END(g, PH_ATTEMPT)
             ++*attempts;
             if (err > 1) {

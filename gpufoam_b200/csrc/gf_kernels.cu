@@ -242,7 +242,7 @@ int launch_lusolve(int n_mats, int m, const double* LU, const int* piv, double* 
 // builds only).
 extern "C" int gf_debug_phase_cycles(unsigned long long* out, int reset) {
     using namespace gf;
-    for (int i = 0; i < 16; ++i) out[i] = 0;
+    for (int i = 0; i < 20; ++i) out[i] = 0;
     phase_cycles_local(out, reset);
     phase_cycles_g1(out, reset);
     phase_cycles_g2(out, reset);
