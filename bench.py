@@ -278,9 +278,9 @@ def main():
     if args.adjoint_only:
         import torch
         torch.cuda.set_device(local)
-        print(json.dumps({"adjoint": adjoint_measure(dict(kind=1, threads_per_cell=128, scratch_in_shared=1,
-                                                          register_budget=1), max(1, args.steps),
-                                                     args.adjoint_cells)}))
+        print(json.dumps({"adjoint": adjoint_measure(dict(kind=1, threads_per_cell=args.threads_per_cell,
+                                                          scratch_in_shared=1, register_budget=args.register_budget),
+                                                     max(1, args.steps), args.adjoint_cells)}))
         return
 
     if args.impl == "reference":

@@ -495,12 +495,15 @@ template <int G, class W>
 __device__ void adj_jacobian_term(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L,
                                   const AdjLayout& A, int y_off, double p, int fbar, int ybar, double* theta_bar) {
     const int nS = M.nS, ld = L.ld;
-    // forward: converted J (L.J), dfdx, the Jacobian terms (stage), then the raw entries
+    // forward: f (A.fs: the recompute's f(y0) at L.dydx0, the same state and
+    // code), the converted J (L.J), dfdx, the Jacobian terms (stage), then the
+    // raw entries; the Jacobian's mixture leaves c, Ha and the third-body
+    // concentrations at y0
     if (g.lane == 0) w[L.scal + S_KCACHE_T] = -1.0;
+    for (int i = g.lane; i < M.m; i += G) w[A.fs + i] = w[L.dydx0 + i];
     g.sync();
     jacobian(g, M, w, L, y_off, p, false);
     stream_gather2(g, M.jst[log2_group(G)], w, L.stage, wa, A.raw);
-    derivatives(g, M, w, L, y_off, p, A.fs);
     adj_mixture(g, M, w, wa, L, A, y_off, p);
     adj_clear_point(g, M, w, wa, A);
     const double CpM = wa[A.ms + MS_CPM], rhoM = wa[A.ms + MS_RHO], alphav = wa[A.ms + MS_AV],
@@ -614,7 +617,8 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
     g.sync();
     {
         GF_PH_BEGIN(g)
-        derivatives(g, M, w, L, L.y0, p, L.dydx0);
+        // f(y0) keeps its rate constants for the Jacobian at the same state
+        derivatives(g, M, w, L, L.y0, p, L.dydx0, true);
         ros_attempt<G, W, true>(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3);
         GF_PH_END(g, PH_ADJ_RECOMPUTE)
     }
@@ -771,8 +775,14 @@ int adjoint_blocks_per_sm(const DevMech& M) {
     const int smem = adjoint_smem_bytes(M);
     if (smem > 227 * 1024) return 0;
     cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+#ifdef GF_ADJ_CARVEOUT
+    cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, GF_ADJ_CARVEOUT);
+#endif
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 64, smem) != cudaSuccess) return 0;
+#ifdef GF_ADJ_BLOCKS
+    per_sm = per_sm < GF_ADJ_BLOCKS ? per_sm : GF_ADJ_BLOCKS;
+#endif
     return per_sm;
 }
 

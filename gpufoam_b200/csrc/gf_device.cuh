@@ -1570,25 +1570,60 @@ __device__ __forceinline__ double ros_d(const RosCoeffs& C, int i) {
     return i == 0 ? C.d1 : (i == 1 ? C.d2 : (i == 2 ? C.d3 : C.d4));
 }
 
+// The Jacobian at y0, I/(gamma dx) - J and its LU (gpuAdaptiveSolver.H:51-73).
+template <int G, class W>
+__device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
+                                            const RosCoeffs& C, int y0_off, double p, double dx) {
+    const int m = M.m;
+    const int ld = L.ld;
+    jacobian(g, M, w, L, y0_off, p, true);
+    {
+        GF_PH_BEGIN(g)
+        shift_and_scale(g, w, L.J, ld, L.vv, m, 1.0 / (C.gamma * dx));
+        GF_PH_END(g, PH_SHIFT)
+    }
+    {
+        GF_PH_BEGIN(g)
+        bool done = false;
+        if constexpr (G >= 32) {
+            if (m <= 64) {
+                lu_decompose_regpanel<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
+                done = true;
+            }
+        }
+        if (!done) lu_decompose_blocked<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
+        GF_PH_END(g, PH_LU)
+    }
+    if (G >= 16) {
+        // the row scaling vv is no longer needed: it holds 1 / U[i][i] from here
+        for (int i = g.lane; i < m; i += G) w[L.vv + i] = 1.0 / w[L.J + i * ld + i];
+        lu_perm(g, w, L.piv, L.perm, m);
+    }
+}
+
 // One attempt solve(y0, dydx0, dx, y) of gpuRosenbrock12/23/34 (their
 // solve(y0, dydx0, dx, y, buffer)); returns the normalised error
 // (normaliseError.H:6-29; the p entry contributes 0). y0 is at y0_off, the
 // candidate is written to yt_off.
 // SAVE (the adjoint sweep): the stage points are kept at save_y2 / save_y3.
-template <int G, class W, bool SAVE = false>
+// F0 (the solve kernel): the attempt also evaluates the step's f(y0) into
+// dydx0 when first_deriv is set (the first attempt of a step), through the
+// stage loop's derivative call: one call site, a smaller instruction
+// footprint. Otherwise the caller provides dydx0.
+template <int G, class W, bool SAVE = false, bool F0 = false>
 __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
                               const OdeParams& o, int y0_off, int yt_off, double p, double dx, int save_y2 = -1,
                               int save_y3 = -1, bool first_deriv = false) {
     const int m = M.m;
     const int ld = L.ld;
+    if constexpr (!F0) factor_step(g, M, w, L, C, y0_off, p, dx);
     // stages: k_i solves (I/(gamma dx) - J) k_i = f_i + dx d_i dfdx + sum_j c_ij k_j / dx,
     // f_0 = f(y0), f_i = f(y0 + sum_j a_ij k_j) where the method takes a new
     // derivative (stage 1; stage 2 of Rosenbrock34), else the previous one.
-    // One loop, so the solve and the derivative each have a single call site:
-    // pass st = -1 evaluates the step's f(y0) (first_deriv: the first attempt
-    // of a step) and then the Jacobian and its LU.
+    // One loop, so the solve and the derivative each have a single call site;
+    // with F0, pass st = -1 evaluates f(y0) (first_deriv) and factors the step.
 #pragma unroll 1
-    for (int st = -1; st < C.s; ++st) {
+    for (int st = F0 ? -1 : 0; st < C.s; ++st) {
         const bool new_f = st < 0 ? first_deriv : (st == 1 || (st == 2 && C.s == 4));
         int at = y0_off, out = L.dydx0;
         if (st > 0 && new_f) {
@@ -1603,31 +1638,11 @@ __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M,
             out = L.dydx;
         }
         if (new_f) derivatives(g, M, w, L, at, p, out, st < 0);
-        if (st < 0) {
-            jacobian(g, M, w, L, y0_off, p, true);
-            {
-                GF_PH_BEGIN(g)
-                shift_and_scale(g, w, L.J, ld, L.vv, m, 1.0 / (C.gamma * dx));
-                GF_PH_END(g, PH_SHIFT)
+        if constexpr (F0) {
+            if (st < 0) {
+                factor_step(g, M, w, L, C, y0_off, p, dx);
+                continue;
             }
-            {
-                GF_PH_BEGIN(g)
-                bool done = false;
-                if constexpr (G >= 32) {
-                    if (m <= 64) {
-                        lu_decompose_regpanel<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
-                        done = true;
-                    }
-                }
-                if (!done) lu_decompose_blocked<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
-                GF_PH_END(g, PH_LU)
-            }
-            if (G >= 16) {
-                // the row scaling vv is no longer needed: it holds 1 / U[i][i] from here
-                for (int i = g.lane; i < m; i += G) w[L.vv + i] = 1.0 / w[L.J + i * ld + i];
-                lu_perm(g, w, L.piv, L.perm, m);
-            }
-            continue;
         }
         const int ki = L.k1 + st * m;
         const int src = st == 0 ? L.dydx0 : L.dydx;
@@ -1699,11 +1714,12 @@ __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, cons
         double dx = step_dxTry;
         double err = 0.0;
         int rejects = 0;
+        // adaptiveSolve's derivatives call before its retry loop
+        // (gpuAdaptiveSolver.H:96): in the solve kernel, inside the first attempt
+        if constexpr (REC) derivatives(g, M, w, L, *y_off, p, L.dydx0, true);
         do {
             GF_PH_BEGIN(g)
-            // the first attempt of the step also evaluates f(y0) (adaptiveSolve's
-            // derivatives call before its retry loop, gpuAdaptiveSolver.H:96)
-            err = ros_attempt(g, M, w, L, C, o, *y_off, *yt_off, p, dx, -1, -1, rejects == 0);
+            err = ros_attempt<G, W, false, !REC>(g, M, w, L, C, o, *y_off, *yt_off, p, dx, -1, -1, rejects == 0);
             GF_PH_END(g, PH_ATTEMPT)
             ++*attempts;
             if (err > 1) {
