@@ -43,12 +43,12 @@ constexpr int kSeedM = 2 * kSideInline, kSeedT = kSeedM + 1, kSeedLnA = kSeedM +
 
 // workspace of the sweep, after the forward workspace of make_layout
 struct AdjLayout {
-    int y2, y3, rb, kb, yb, fb0, fb2, fb3, fs, Jb, raw, cb, Mb, gq, ms, vb, dn, ab, dd, size;
+    int y2, y3, rb, kb, yb, fb0, fb2, fb3, fs, f2, f3, Jb, raw, cb, Mb, gq, ms, vb, dn, ab, dd, size;
 };
 enum { MS_RHO = 0, MS_CPM, MS_DCPM, MS_AV, MS_RHOB, MS_CPMB, MS_DCPMB, MS_AVB, MS_TB, MS_SH, MS_N = 16 };
 
-// y2, y3 and fs live in the forward workspace (shared memory), after its
-// make_layout part (fwd_size doubles in all); every other array is in the
+// y2, y3, fs, f2 and f3 live in the forward workspace (shared memory), after
+// its make_layout part (fwd_size doubles in all); every other array is in the
 // per-CTA adjoint region in global memory, offsets from 0.
 __host__ __device__ inline AdjLayout make_adj_layout(const WsLayout& L, int nS, int nR, int n_tb, int* fwd_size) {
     const int m = nS + 1;
@@ -56,7 +56,9 @@ __host__ __device__ inline AdjLayout make_adj_layout(const WsLayout& L, int nS, 
     A.y2 = L.size;
     A.y3 = L.size + m;
     A.fs = L.size + 2 * m;            // f at the point being reversed
-    *fwd_size = L.size + 3 * m;
+    A.f2 = L.size + 3 * m;            // f at the stage points, from the recompute
+    A.f3 = L.size + 4 * m;
+    *fwd_size = L.size + 5 * m;
     int o = 0;
     A.rb = o; o += 4 * m;
     A.kb = o; o += 4 * m;
@@ -474,9 +476,14 @@ __device__ void adj_clear_point(const Grp<G>& g, const DevMech& M, const W& w, c
 // ybar += (df/dy)^T fbar at the point y (no Jacobian term)
 template <int G, class W>
 __device__ void adj_vjp_f(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L, const AdjLayout& A,
-                          int y_off, double p, int fbar, int ybar, double* theta_bar) {
-    derivatives(g, M, w, L, y_off, p, A.fs);  // f, c, Ha and the third-body concentrations at y
-    adj_mixture(g, M, w, wa, L, A, y_off, p);     // + Cp, v, rhoM/W and the scalars
+                          int y_off, double p, int f_off, int fbar, int ybar, double* theta_bar) {
+    // f at y: the recompute's value (f_off; the same state and code)
+    for (int i = g.lane; i < M.m; i += G) w[A.fs + i] = w[f_off + i];
+    adj_mixture(g, M, w, wa, L, A, y_off, p);     // c, Ha, Cp, v, rhoM/W and the scalars at y
+    if (M.n_tb > 0) {
+        third_body_all(g, M, w, L.c, L.Mtb);          // the third-body concentrations at y
+        g.sync();
+    }
     adj_clear_point(g, M, w, wa, A);
     adj_rhs_assembly(g, M, w, wa, L, A, fbar);
     {
@@ -619,7 +626,7 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
         GF_PH_BEGIN(g)
         // f(y0) keeps its rate constants for the Jacobian at the same state
         derivatives(g, M, w, L, L.y0, p, L.dydx0, true);
-        ros_attempt<G, W, true>(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3);
+        ros_attempt<G, W, true>(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3, false, A.f2, A.f3);
         GF_PH_END(g, PH_ADJ_RECOMPUTE)
     }
     // kbar_i = b_i ybar; the ybar of y1 = y0 + sum b_i k_i flows to y0 unchanged
@@ -655,7 +662,7 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
             g.sync();
             {
                 GF_PH_BEGIN(g)
-                adj_vjp_f(g, M, w, wa, L, A, pt, p, fb, A.ab, theta_bar);
+                adj_vjp_f(g, M, w, wa, L, A, pt, p, st == 1 ? A.f2 : A.f3, fb, A.ab, theta_bar);
                 GF_PH_END(g, PH_ADJ_VJP)
             }
             for (int i = g.lane; i < m; i += G) {

@@ -1605,7 +1605,8 @@ __device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, c
 // solve(y0, dydx0, dx, y, buffer)); returns the normalised error
 // (normaliseError.H:6-29; the p entry contributes 0). y0 is at y0_off, the
 // candidate is written to yt_off.
-// SAVE (the adjoint sweep): the stage points are kept at save_y2 / save_y3.
+// SAVE (the adjoint sweep): the stage points are kept at save_y2 / save_y3
+// and f at them at save_f2 / save_f3.
 // F0 (the solve kernel): the attempt also evaluates the step's f(y0) into
 // dydx0 when first_deriv is set (the first attempt of a step), through the
 // stage loop's derivative call: one call site, a smaller instruction
@@ -1613,7 +1614,7 @@ __device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, c
 template <int G, class W, bool SAVE = false, bool F0 = false>
 __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
                               const OdeParams& o, int y0_off, int yt_off, double p, double dx, int save_y2 = -1,
-                              int save_y3 = -1, bool first_deriv = false) {
+                              int save_y3 = -1, bool first_deriv = false, int save_f2 = -1, int save_f3 = -1) {
     const int m = M.m;
     const int ld = L.ld;
     if constexpr (!F0) factor_step(g, M, w, L, C, y0_off, p, dx);
@@ -1638,6 +1639,12 @@ __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M,
             out = L.dydx;
         }
         if (new_f) derivatives(g, M, w, L, at, p, out, st < 0);
+        if constexpr (SAVE) {
+            if (st > 0 && new_f) {
+                const int fs = st == 1 ? save_f2 : save_f3;
+                for (int i = g.lane; i < m; i += G) w[fs + i] = w[L.dydx + i];
+            }
+        }
         if constexpr (F0) {
             if (st < 0) {
                 factor_step(g, M, w, L, C, y0_off, p, dx);
