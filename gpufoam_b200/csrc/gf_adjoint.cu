@@ -43,7 +43,7 @@ constexpr int kSeedM = 2 * kSideInline, kSeedT = kSeedM + 1, kSeedLnA = kSeedM +
 
 // workspace of the sweep, after the forward workspace of make_layout
 struct AdjLayout {
-    int y2, y3, rb, kb, yb, fb0, fb2, fb3, fs, f2, f3, Jb, raw, cb, Mb, gq, ms, vb, dn, ab, dd, size;
+    int y2, y3, rb, kb, yb, fb0, fb2, fb3, fs, f2, f3, Jb, raw, Jc, dfc, cb, Mb, gq, ms, vb, dn, ab, dd, size;
 };
 enum { MS_RHO = 0, MS_CPM, MS_DCPM, MS_AV, MS_RHOB, MS_CPMB, MS_DCPMB, MS_AVB, MS_TB, MS_SH, MS_N = 16 };
 
@@ -68,6 +68,8 @@ __host__ __device__ inline AdjLayout make_adj_layout(const WsLayout& L, int nS, 
     A.fb3 = o; o += m;
     A.Jb = o; o += m * L.ld;
     A.raw = o; o += m * L.ld;
+    A.Jc = o; o += m * L.ld;          // the converted Jacobian at y0 (before the shift)
+    A.dfc = o; o += m;                // its dfdx
     A.cb = o; o += nS;
     A.Mb = o; o += (n_tb > 0 ? n_tb : 1);
     A.gq = o; o += 2 * kSideInline * (nR > 0 ? nR : 1);
@@ -502,16 +504,19 @@ template <int G, class W>
 __device__ void adj_jacobian_term(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const WsLayout& L,
                                   const AdjLayout& A, int y_off, double p, int fbar, int ybar, double* theta_bar) {
     const int nS = M.nS, ld = L.ld;
-    // forward: f (A.fs: the recompute's f(y0) at L.dydx0, the same state and
-    // code), the converted J (L.J), dfdx, the Jacobian terms (stage), then the
-    // raw entries; the Jacobian's mixture leaves c, Ha and the third-body
-    // concentrations at y0
-    if (g.lane == 0) w[L.scal + S_KCACHE_T] = -1.0;
-    for (int i = g.lane; i < M.m; i += G) w[A.fs + i] = w[L.dydx0 + i];
-    g.sync();
-    jacobian(g, M, w, L, y_off, p, false);
-    stream_gather2(g, M.jst[log2_group(G)], w, L.stage, wa, A.raw);
+    // forward at y0, all from the recompute (the same state and code): f
+    // (L.dydx0), the converted J and dfdx (A.Jc, A.dfc), the raw entries
+    // (A.raw); the mixture and the third-body concentrations are evaluated again
+    for (int i = g.lane; i < M.m; i += G) {
+        w[A.fs + i] = w[L.dydx0 + i];
+        w[L.dfdx + i] = wa[A.dfc + i];
+    }
+    for (int e = g.lane; e < M.m * ld; e += G) w[L.J + e] = wa[A.Jc + e];
     adj_mixture(g, M, w, wa, L, A, y_off, p);
+    if (M.n_tb > 0) {
+        third_body_all(g, M, w, L.c, L.Mtb);
+        g.sync();
+    }
     adj_clear_point(g, M, w, wa, A);
     const double CpM = wa[A.ms + MS_CPM], rhoM = wa[A.ms + MS_RHO], alphav = wa[A.ms + MS_AV],
                  dCpMdT = wa[A.ms + MS_DCPM];
@@ -626,6 +631,14 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
         GF_PH_BEGIN(g)
         // f(y0) keeps its rate constants for the Jacobian at the same state
         derivatives(g, M, w, L, L.y0, p, L.dydx0, true);
+        jacobian(g, M, w, L, L.y0, p, true);
+        // kept for the Jacobian term: the raw entries (from the Jacobian terms
+        // in the staging slots), the converted Jacobian and dfdx
+        stream_gather2(g, M.jst[log2_group(G)], w, L.stage, wa, A.raw);
+        for (int e = g.lane; e < m * ld; e += G) wa[A.Jc + e] = w[L.J + e];
+        for (int i = g.lane; i < m; i += G) wa[A.dfc + i] = w[L.dfdx + i];
+        g.sync();
+        shift_and_factor(g, M, w, L, C, h);
         ros_attempt<G, W, true>(g, M, w, L, C, o, L.y0, L.yt, p, h, A.y2, A.y3, false, A.f2, A.f3);
         GF_PH_END(g, PH_ADJ_RECOMPUTE)
     }

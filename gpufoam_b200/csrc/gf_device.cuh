@@ -1570,13 +1570,12 @@ __device__ __forceinline__ double ros_d(const RosCoeffs& C, int i) {
     return i == 0 ? C.d1 : (i == 1 ? C.d2 : (i == 2 ? C.d3 : C.d4));
 }
 
-// The Jacobian at y0, I/(gamma dx) - J and its LU (gpuAdaptiveSolver.H:51-73).
+// I/(gamma dx) - J of the Jacobian in L.J, and its LU (gpuAdaptiveSolver.H:51-73).
 template <int G, class W>
-__device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
-                                            const RosCoeffs& C, int y0_off, double p, double dx) {
+__device__ __forceinline__ void shift_and_factor(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
+                                                 const RosCoeffs& C, double dx) {
     const int m = M.m;
     const int ld = L.ld;
-    jacobian(g, M, w, L, y0_off, p, true);
     {
         GF_PH_BEGIN(g)
         shift_and_scale(g, w, L.J, ld, L.vv, m, 1.0 / (C.gamma * dx));
@@ -1601,12 +1600,21 @@ __device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, c
     }
 }
 
+// The Jacobian at y0, then shift_and_factor.
+template <int G, class W>
+__device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
+                                            const RosCoeffs& C, int y0_off, double p, double dx) {
+    jacobian(g, M, w, L, y0_off, p, true);
+    shift_and_factor(g, M, w, L, C, dx);
+}
+
 // One attempt solve(y0, dydx0, dx, y) of gpuRosenbrock12/23/34 (their
 // solve(y0, dydx0, dx, y, buffer)); returns the normalised error
 // (normaliseError.H:6-29; the p entry contributes 0). y0 is at y0_off, the
 // candidate is written to yt_off.
-// SAVE (the adjoint sweep): the stage points are kept at save_y2 / save_y3
-// and f at them at save_f2 / save_f3.
+// SAVE (the adjoint sweep): the caller has factored the step (L.J holds the
+// LU); the stage points are kept at save_y2 / save_y3 and f at them at
+// save_f2 / save_f3.
 // F0 (the solve kernel): the attempt also evaluates the step's f(y0) into
 // dydx0 when first_deriv is set (the first attempt of a step), through the
 // stage loop's derivative call: one call site, a smaller instruction
@@ -1617,7 +1625,7 @@ __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M,
                               int save_y3 = -1, bool first_deriv = false, int save_f2 = -1, int save_f3 = -1) {
     const int m = M.m;
     const int ld = L.ld;
-    if constexpr (!F0) factor_step(g, M, w, L, C, y0_off, p, dx);
+    if constexpr (!F0 && !SAVE) factor_step(g, M, w, L, C, y0_off, p, dx);
     // stages: k_i solves (I/(gamma dx) - J) k_i = f_i + dx d_i dfdx + sum_j c_ij k_j / dx,
     // f_0 = f(y0), f_i = f(y0 + sum_j a_ij k_j) where the method takes a new
     // derivative (stage 1; stage 2 of Rosenbrock34), else the previous one.
