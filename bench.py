@@ -64,6 +64,12 @@ WORKLOADS = {
     "gri30-100k": dict(mech="gri30", n=100_000, dT=1e-6, T=(1000.0, 2500.0)),
 }
 DTC0 = 1e-7
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of the
+# persistent kernel on the GRI-size mechanism, from one ncu capture of 4 096
+# cells (threads_per_cell 64, shared-memory workspace): 2 481 152 B read, 0 B
+# written (the outputs were still in L2 when the launch ended). Scaled by the
+# cell count for the same kernel on the larger GRI-size batches.
+NCU_DRAM_BYTES_PER_CELL_GRI = 2481152 / 4096
 
 
 def parse():
@@ -505,7 +511,12 @@ def main():
                            deltaTChem0=DTC0, launch=solver.get_launch(), l2="inputs larger than L2 (not flushed)",
                            parallelism=f"cells sharded over {world} GPU(s)"),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                         "frac": achieved / peak.value, "traffic": None,
+                         "frac": achieved / peak.value,
+                         "traffic": (NCU_DRAM_BYTES_PER_CELL_GRI * n
+                                     if wl.get("mech") == "gri" and solver.get_launch()["threads_per_cell"] == 64
+                                     else None),
+                         "traffic_source": "ncu dram bytes of 4096 GRI-size cells, scaled per cell",
+                         "algorithmic_bytes_per_launch": int(n * 2 * cells.shape[1] * 8),
                          "peak_source": "measured DFMA microbenchmark on this GPU (gf_measure_fp64_peak)",
                          "algorithmic_flop_per_launch": flop, "attempts": attempts, "accepted": accepted},
             "plain": plain,
