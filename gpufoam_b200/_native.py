@@ -31,7 +31,7 @@ EXPORTS = [
     "gf_strerror", "gf_abi_version", "gf_last_cuda_error", "gf_measure_fp64_peak", "gf_solve_noalloc",
     "gf_solve_record", "gf_adjoint", "gf_solve_graph_create", "gf_solve_graph_set_delta_t",
     "gf_solve_graph_launch", "gf_solve_graph_stats", "gf_solve_graph_destroy", "gf_cell_rates",
-    "gf_reaction_rates", "gf_qdot",
+    "gf_reaction_rates", "gf_qdot", "gf_gather_states", "gf_scatter_rates",
 ]
 
 
@@ -140,6 +140,8 @@ def load() -> C.CDLL:
     lib.gf_cell_rates.argtypes = [vp, ip, vp, vp, ip, vp, ip, vp, vp]
     lib.gf_reaction_rates.argtypes = [vp, ip, ip, vp, vp, ip, vp, vp, ip, vp]
     lib.gf_qdot.argtypes = [vp, ip, vp, ip, vp, vp]
+    lib.gf_gather_states.argtypes = [ip, ip, P(vp), vp, vp, vp, ip, vp]
+    lib.gf_scatter_rates.argtypes = [ip, ip, vp, ip, P(vp), vp]
     lib.gf_strerror.argtypes = [ip]
     lib.gf_strerror.restype = C.c_char_p
     lib.gf_abi_version.restype = ip

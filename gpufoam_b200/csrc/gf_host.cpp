@@ -889,6 +889,32 @@ void gf_solve_graph_destroy(gf_solve_graph* g) {
     delete g;
 }
 
+// ---- the plugin's field gather and rate scatter (gf_fieldio.cu) --------------
+
+int gf_gather_states(int n_cells, int n_species, const double* const* Y_fields, const double* T, const double* p,
+                     double* y, int ld_y, void* stream) {
+    if (n_cells < 0 || n_species < 1 || n_species > GF_MAX_SPECIES || ld_y < n_species + 2 || !Y_fields)
+        return GF_ERR_INVALID_ARGUMENT;
+    if (n_cells == 0) return GF_OK;
+    if (!T || !p || !y) return GF_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n_species; ++i)
+        if (!Y_fields[i]) return GF_ERR_INVALID_ARGUMENT;
+    const int e = gf::launch_gather_states(n_cells, n_species, Y_fields, T, p, y, ld_y, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
+}
+
+int gf_scatter_rates(int n_cells, int n_species, const double* RR, int ld_rr, double* const* RR_fields,
+                     void* stream) {
+    if (n_cells < 0 || n_species < 1 || n_species > GF_MAX_SPECIES || ld_rr < n_species || !RR_fields)
+        return GF_ERR_INVALID_ARGUMENT;
+    if (n_cells == 0) return GF_OK;
+    if (!RR) return GF_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n_species; ++i)
+        if (!RR_fields[i]) return GF_ERR_INVALID_ARGUMENT;
+    const int e = gf::launch_scatter_rates(n_cells, n_species, RR, ld_rr, RR_fields, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
+}
+
 // ---- the plugin's per-cell side paths (gf_fields.cu) --------------------------
 
 int gf_cell_rates(const gf_mech* m, int n_cells, const double* rho, const double* y, int ld_y, double* RR,

@@ -202,6 +202,11 @@ struct FieldArgs {
 int launch_cell_fields(const DevMech& m, const FieldArgs& a, void* stream);
 int launch_qdot(const DevMech& m, int n_cells, const double* RR, int ld_rr, double* qdot, void* stream);
 
+// The plugin's field gather and rate scatter (gf_fieldio.cu).
+int launch_gather_states(int n, int nS, const double* const* Y, const double* T, const double* p, double* y, int ld,
+                         void* stream);
+int launch_scatter_rates(int n, int nS, const double* RR, int ld, double* const* out, void* stream);
+
 // Device tables of a mechanism object (gf_host.cpp).
 const DevMech* mech_device_tables(const gf_mech* m);
 

@@ -438,3 +438,28 @@ def qdot(mech: Mechanism, RR):
     out = torch.empty(rd.shape[0], dtype=torch.float64, device="cuda")
     N.check(mech.lib.gf_qdot(mech.handle, rd.shape[0], _ptr(rd), rd.shape[1], _ptr(out), _stream_ptr()), "gf_qdot")
     return out
+
+
+# ---- the plugin's field gather and rate scatter (gpuChemistryModel.C:33-53, :351-356), on the GPU
+
+def gather_states(Y_fields, T, p, ld: Optional[int] = None):
+    """Per-species fields (a sequence of nS cuda tensors of n cells) plus T and p ->
+    the cell-major states [n][ld] (ld >= nS + 2) that gf_solve takes."""
+    import torch
+    nS = len(Y_fields)
+    n = int(T.shape[0])
+    ld = ld or nS + 2
+    y = torch.zeros((n, ld), dtype=torch.float64, device="cuda")
+    ptrs = (C.c_void_p * max(nS, 1))(*[f.data_ptr() for f in Y_fields])
+    lib = N.load()
+    N.check(lib.gf_gather_states(n, nS, ptrs, _ptr(T), _ptr(p), _ptr(y), ld, _stream_ptr()), "gf_gather_states")
+    return y
+
+
+def scatter_rates(RR, RR_fields):
+    """Cell-major rates RR [n][>= nS] -> the per-species fields RR_fields (nS cuda tensors of n)."""
+    nS = len(RR_fields)
+    ptrs = (C.c_void_p * max(nS, 1))(*[f.data_ptr() for f in RR_fields])
+    lib = N.load()
+    N.check(lib.gf_scatter_rates(int(RR.shape[0]), nS, _ptr(RR), int(RR.shape[1]), ptrs, _stream_ptr()),
+            "gf_scatter_rates")

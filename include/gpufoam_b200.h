@@ -247,6 +247,22 @@ int gf_compute_ynew(gf_solver* solver, int n_cells, double deltaT, double deltaT
                     const double* deltaTChem, const double* Y, double* Ynew,
                     double* deltaTChemNew);
 
+/* ---- the plugin's field gather and rate scatter ---------------------------
+ * The plugin packs OpenFOAM's per-species fields into cell-major states on the
+ * host (getY0, gpu_chemistry/src/gpuChemistryModels/gpuChemistryModel/
+ * gpuChemistryModel.C:33-53) and unpacks the cell-major rates into per-species
+ * fields after the solve (computeRRAndChemDeltaT, gpuChemistryModel.C:351-356).
+ * With the fields in device memory both run on the GPU. Y_fields and RR_fields
+ * are host arrays of n_species device pointers (one field of n_cells values
+ * each); 1 <= n_species <= GF_MAX_SPECIES.
+ *   gf_gather_states   y[c][i] = Y_fields[i][c], y[c][nS] = T[c], y[c][nS+1] = p[c]
+ *                      (row stride ld_y >= n_species + 2)
+ *   gf_scatter_rates   RR_fields[i][c] = RR[c][i] (row stride ld_rr >= n_species) */
+int gf_gather_states(int n_cells, int n_species, const double* const* Y_fields, const double* T,
+                     const double* p, double* y, int ld_y, void* stream);
+int gf_scatter_rates(int n_cells, int n_species, const double* RR, int ld_rr, double* const* RR_fields,
+                     void* stream);
+
 /* ---- the plugin's per-cell side paths ------------------------------------
  * gpuChemistryModel computes these on the CPU through OpenFOAM's reactions
  * (gpu_chemistry/src/gpuChemistryModels/gpuChemistryModel/gpuChemistryModel.C);
