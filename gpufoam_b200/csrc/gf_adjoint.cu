@@ -795,14 +795,8 @@ int adjoint_blocks_per_sm(const DevMech& M) {
     const int smem = adjoint_smem_bytes(M);
     if (smem > 227 * 1024) return 0;
     cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-#ifdef GF_ADJ_CARVEOUT
-    cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, GF_ADJ_CARVEOUT);
-#endif
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, 64, smem) != cudaSuccess) return 0;
-#ifdef GF_ADJ_BLOCKS
-    per_sm = per_sm < GF_ADJ_BLOCKS ? per_sm : GF_ADJ_BLOCKS;
-#endif
     return per_sm;
 }
 
