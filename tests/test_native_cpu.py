@@ -91,3 +91,19 @@ def test_ode_input_defaults():
 def test_is_integer_rule():
     # isInteger truncates toward zero and only rejects a positive remainder
     assert E.is_integer(2.0) and E.is_integer(-0.5) and not E.is_integer(1.5)
+
+
+def test_null_handles_rejected_without_a_device(lib):
+    """Entry points added around the solve reject missing handles before any
+    CUDA call (no GPU needed)."""
+    st = N.GfStats()
+    out = C.c_void_p()
+    assert lib.gf_solve_graph_create(None, 4, 1e-6, None, 1.0, None, None, None, 12, None, None, None, 0, None,
+                                     None, C.byref(out)) == 1
+    assert lib.gf_solve_graph_launch(None, None) == 1
+    assert lib.gf_solve_graph_set_delta_t(None, 1e-6) == 1
+    assert lib.gf_solve_graph_stats(None, C.byref(st)) == 1
+    lib.gf_solve_graph_destroy(None)
+    assert lib.gf_cell_rates(None, 4, None, None, 12, None, 10, None, None) == 1
+    assert lib.gf_reaction_rates(None, 4, 0, None, None, 12, None, None, 10, None) == 1
+    assert lib.gf_qdot(None, 4, None, 10, None, None) == 1
