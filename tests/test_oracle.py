@@ -149,6 +149,28 @@ def test_port_vs_reference_live(factory, seed):
 
 
 @needs_ref
+@pytest.mark.parametrize("name", CASES)
+def test_side_paths_port_vs_reference(name):
+    """calculate / tc / reactionRR / specieReactionRR / Qdot (gpuChemistryModel.C:145-450):
+    the C restatement against the reference's own reaction objects, bit for bit,
+    including a state with all concentrations zero (tc = vGreat)."""
+    g = load(name)
+    mech = fixture_mech(g)
+    a, b = Oracle(mech, "port"), Oracle(mech, "reference")
+    y = np.vstack([g["states"], M.make_cells(mech, 4, seed=7, T_range=(250.0, 3500.0))])
+    rho = np.linspace(0.05, 3.0, y.shape[0])
+    rho[-1] = 0.0
+    RRa, tca = a.cell_fields(rho, y)
+    RRb, tcb = b.cell_fields(rho, y)
+    assert eq(RRa, RRb) and eq(tca, tcb)
+    assert tca[-1] == np.finfo(np.float64).max / 10
+    assert eq(a.qdot(RRa), b.qdot(RRb))
+    for r in range(0, mech.n_reactions, max(1, mech.n_reactions // 17)):
+        for x, z in zip(a.reaction_fields(r, rho, y), b.reaction_fields(r, rho, y)):
+            assert eq(x, z)
+
+
+@needs_ref
 def test_reference_counted_wrapper_matches_reference_functor():
     """The counting wrapper used for step counts gives the same states as the
     reference's own singleCellSolver functor."""
