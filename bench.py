@@ -88,6 +88,9 @@ def parse():
     ap.add_argument("--register-budget", type=int, default=0, choices=[0, 1],
                     help="persistent kernel: 0 = up to 255 registers per thread, 1 = at most 128")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="timed steps of the plain-kernel leg (at most --steps; one warm-up step before). "
+                         "The plain kernel runs ~10x longer than the persistent one on mixed batches")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -416,7 +419,7 @@ def main():
     if not args.no_plain:
         ps = E.Solver(mechs, ode)
         ps.set_launch(kind=0)
-        pms, pcnt, _ = timed(ps, max(1, min(args.steps, 2)), 1)
+        pms, pcnt, _ = timed(ps, max(1, min(args.steps, args.plain_steps)), 1)
         pm = float(np.mean(pms))
         if world > 1:
             t = torch.tensor([pm], dtype=torch.float64, device="cuda")
