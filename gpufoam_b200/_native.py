@@ -31,7 +31,7 @@ EXPORTS = [
     "gf_strerror", "gf_abi_version", "gf_last_cuda_error", "gf_measure_fp64_peak", "gf_solve_noalloc",
     "gf_solve_record", "gf_adjoint", "gf_solve_graph_create", "gf_solve_graph_set_delta_t",
     "gf_solve_graph_launch", "gf_solve_graph_stats", "gf_solve_graph_destroy", "gf_cell_rates",
-    "gf_reaction_rates", "gf_qdot", "gf_gather_states", "gf_scatter_rates",
+    "gf_reaction_rates", "gf_qdot", "gf_gather_states", "gf_scatter_rates", "gf_compute_rr_lts",
 ]
 
 
@@ -122,6 +122,7 @@ def load() -> C.CDLL:
     lib.gf_solve.argtypes = [vp, ip, dp, vp, dp, vp, vp, vp, ip, vp, vp, vp, ip, vp, vp, P(GfStats), vp]
     lib.gf_compute_rr.argtypes = [vp, ip, dp, dp, vp, vp, vp, vp, vp, P(dp)]
     lib.gf_compute_ynew.argtypes = [vp, ip, dp, dp, vp, vp, vp, vp]
+    lib.gf_compute_rr_lts.argtypes = [vp, ip, vp, dp, vp, vp, vp, vp, vp, P(dp)]
     lib.gf_rates.argtypes = [vp, ip, vp, vp, vp]
     lib.gf_jacobian.argtypes = [vp, ip, vp, vp, vp, vp]
     lib.gf_lu_decompose.argtypes = [ip, ip, vp, vp, vp]

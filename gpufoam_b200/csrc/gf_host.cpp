@@ -174,6 +174,7 @@ struct gf_solver {
     double* dRR = nullptr;
     double* drho = nullptr;
     double* ddtc = nullptr;
+    double* ddt = nullptr;  // per-cell flow time steps (local time stepping)
     int staged_cells = 0;
 };
 
@@ -200,7 +201,8 @@ int ensure_staging(gf_solver* s, int n) {
     cudaFree(s->dRR);
     cudaFree(s->drho);
     cudaFree(s->ddtc);
-    s->dY = s->dYnew = s->dRR = s->drho = s->ddtc = nullptr;
+    cudaFree(s->ddt);
+    s->dY = s->dYnew = s->dRR = s->drho = s->ddtc = s->ddt = nullptr;
     s->staged_cells = 0;
     const size_t ne = (size_t)s->max_neq;
     GF_CUDA(cudaMalloc(&s->dY, (size_t)n * ne * sizeof(double)));
@@ -208,6 +210,7 @@ int ensure_staging(gf_solver* s, int n) {
     GF_CUDA(cudaMalloc(&s->dRR, (size_t)n * ne * sizeof(double)));
     GF_CUDA(cudaMalloc(&s->drho, (size_t)n * sizeof(double)));
     GF_CUDA(cudaMalloc(&s->ddtc, (size_t)n * sizeof(double)));
+    GF_CUDA(cudaMalloc(&s->ddt, (size_t)n * sizeof(double)));
     s->staged_cells = n;
     return GF_OK;
 }
@@ -631,6 +634,7 @@ void gf_solver_destroy(gf_solver* s) {
     cudaFree(s->dRR);
     cudaFree(s->drho);
     cudaFree(s->ddtc);
+    cudaFree(s->ddt);
     delete s;
 }
 
@@ -1005,8 +1009,8 @@ int gf_adjoint(gf_solver* s, int n_cells, const double* traj, int traj_cap, cons
     return e ? cuda_fail((cudaError_t)e) : GF_OK;
 }
 
-static int host_solve(gf_solver* s, int n, double deltaT, double deltaTChemMax, const double* rho,
-                      const double* deltaTChem, const double* Y, double* Ynew_out, double* RR_out,
+static int host_solve(gf_solver* s, int n, double deltaT, const double* deltaT_cell, double deltaTChemMax,
+                      const double* rho, const double* deltaTChem, const double* Y, double* Ynew_out, double* RR_out,
                       double* deltaTChemNew, double* minDeltaT) {
     if (!s || n < 0 || !deltaTChem || !Y || !deltaTChemNew || s->mechs.size() != 1) return GF_ERR_INVALID_ARGUMENT;
     if (n == 0) return GF_OK;
@@ -1016,9 +1020,11 @@ static int host_solve(gf_solver* s, int n, double deltaT, double deltaTChemMax, 
     GF_CUDA(cudaMemcpyAsync(s->dY, Y, (size_t)n * ne * sizeof(double), cudaMemcpyHostToDevice, 0));
     GF_CUDA(cudaMemcpyAsync(s->ddtc, deltaTChem, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, 0));
     if (RR_out) GF_CUDA(cudaMemcpyAsync(s->drho, rho, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, 0));
+    if (deltaT_cell)
+        GF_CUDA(cudaMemcpyAsync(s->ddt, deltaT_cell, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, 0));
     gf_stats st;
-    r = gf_solve(s, n, deltaT, nullptr, deltaTChemMax, nullptr, RR_out ? s->drho : nullptr, s->dY, ne, s->dYnew,
-                 s->ddtc, RR_out ? s->dRR : nullptr, nS, nullptr, nullptr, &st, 0);
+    r = gf_solve(s, n, deltaT, deltaT_cell ? s->ddt : nullptr, deltaTChemMax, nullptr, RR_out ? s->drho : nullptr,
+                 s->dY, ne, s->dYnew, s->ddtc, RR_out ? s->dRR : nullptr, nS, nullptr, nullptr, &st, 0);
     if (r) return r;
     if (Ynew_out) GF_CUDA(cudaMemcpy(Ynew_out, s->dYnew, (size_t)n * ne * sizeof(double), cudaMemcpyDeviceToHost));
     if (RR_out) GF_CUDA(cudaMemcpy(RR_out, s->dRR, (size_t)n * nS * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1031,7 +1037,17 @@ static int host_solve(gf_solver* s, int n, double deltaT, double deltaTChemMax, 
 int gf_compute_rr(gf_solver* s, int n, double deltaT, double deltaTChemMax, const double* rho,
                   const double* deltaTChem, const double* Y, double* RR, double* deltaTChemNew, double* minDeltaT) {
     if (!rho || !RR) return GF_ERR_INVALID_ARGUMENT;
-    return host_solve(s, n, deltaT, deltaTChemMax, rho, deltaTChem, Y, nullptr, RR, deltaTChemNew, minDeltaT);
+    return host_solve(s, n, deltaT, nullptr, deltaTChemMax, rho, deltaTChem, Y, nullptr, RR, deltaTChemNew,
+                      minDeltaT);
+}
+
+// computeRR with a flow time step per cell: the local time stepping that
+// gpuChemistryModel::solve(const scalarField&) rejects (gpuChemistryModel.C:328-333).
+int gf_compute_rr_lts(gf_solver* s, int n, const double* deltaT, double deltaTChemMax, const double* rho,
+                      const double* deltaTChem, const double* Y, double* RR, double* deltaTChemNew,
+                      double* minDeltaT) {
+    if (!rho || !RR || (n > 0 && !deltaT)) return GF_ERR_INVALID_ARGUMENT;
+    return host_solve(s, n, 0.0, deltaT, deltaTChemMax, rho, deltaTChem, Y, nullptr, RR, deltaTChemNew, minDeltaT);
 }
 
 // GpuKernelEvaluator::computeYNew (gpuKernelEvaluator.cu:35-63): deltaTChemNew unclamped
@@ -1039,7 +1055,8 @@ int gf_compute_ynew(gf_solver* s, int n, double deltaT, double deltaTChemMax, co
                     const double* Y, double* Ynew, double* deltaTChemNew) {
     (void)deltaTChemMax;
     if (!Ynew) return GF_ERR_INVALID_ARGUMENT;
-    return host_solve(s, n, deltaT, INFINITY, nullptr, deltaTChem, Y, Ynew, nullptr, deltaTChemNew, nullptr);
+    return host_solve(s, n, deltaT, nullptr, INFINITY, nullptr, deltaTChem, Y, Ynew, nullptr, deltaTChemNew,
+                      nullptr);
 }
 
 int gf_rates(const gf_mech* m, int n, const double* y, double* dydx, void* stream) {

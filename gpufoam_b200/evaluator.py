@@ -338,6 +338,25 @@ class GpuKernelEvaluator:
                                        C.byref(mn)), "gf_compute_rr")
         return RR, dtn, mn.value
 
+    def computeRRLocal(self, deltaT, deltaTChemMax: float, rho, deltaTChem, Y):
+        """computeRR with a flow time step per cell, deltaT [nCells] (local time
+        stepping; the reference's solve(const scalarField&) throws,
+        gpuChemistryModel.C:328-333) -> (RR, deltaTChemNew clamped, minDeltaT)."""
+        dT = np.ascontiguousarray(deltaT, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        dtc = np.ascontiguousarray(deltaTChem, dtype=np.float64)
+        Yh = np.ascontiguousarray(Y, dtype=np.float64).reshape(-1)
+        n = rho.shape[0]
+        if dT.shape != (n,):
+            raise ValueError("deltaT must hold one value per cell")
+        RR = np.empty(n * self.nSpecie)
+        dtn = np.empty(n)
+        mn = C.c_double()
+        N.check(self.lib.gf_compute_rr_lts(self.solver.handle, n, dT.ctypes.data, float(deltaTChemMax),
+                                           rho.ctypes.data, dtc.ctypes.data, Yh.ctypes.data, RR.ctypes.data,
+                                           dtn.ctypes.data, C.byref(mn)), "gf_compute_rr_lts")
+        return RR, dtn, mn.value
+
 
 def solve_noalloc(mech: Mechanism, ode: OdeInputs, Y0, deltaT: float, deltaTChem, Ynew, Treact: float = 0.0,
                   deltaTChemMax: float = np.inf, rho=None, RR=None, status=None, counters=None, stats=True,

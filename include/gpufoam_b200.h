@@ -241,6 +241,14 @@ int gf_compute_rr(gf_solver* solver, int n_cells, double deltaT, double deltaTCh
                   const double* rho, const double* deltaTChem, const double* Y,
                   double* RR, double* deltaTChemNew, double* minDeltaT);
 
+/* gf_compute_rr with a flow time step per cell, deltaT [n_cells] (host): the
+ * local time stepping that gpuChemistryModel::solve(const scalarField& deltaT)
+ * rejects in the reference (gpuChemistryModel.C:328-333). RR uses each cell's
+ * own deltaT. */
+int gf_compute_rr_lts(gf_solver* solver, int n_cells, const double* deltaT, double deltaTChemMax,
+                      const double* rho, const double* deltaTChem, const double* Y,
+                      double* RR, double* deltaTChemNew, double* minDeltaT);
+
 /* Host-memory mirror of GpuKernelEvaluator::computeYNew: Ynew [n_cells][nEqns]
  * and deltaTChemNew [n_cells] (not clamped, as in the reference). */
 int gf_compute_ynew(gf_solver* solver, int n_cells, double deltaT, double deltaTChemMax,

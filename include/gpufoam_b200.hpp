@@ -98,6 +98,23 @@ public:
         return std::make_tuple(std::move(RR), std::move(dtc), minDeltaT);
     }
 
+    // computeRR with a flow time step per cell (local time stepping; the
+    // reference's solve(const scalarField&) throws, gpuChemistryModel.C:328-333)
+    std::tuple<std::vector<double>, std::vector<double>, double> computeRR(const std::vector<double>& deltaT,
+                                                                           double deltaTChemMax,
+                                                                           const std::vector<double>& rho,
+                                                                           const std::vector<double>& deltaTChem,
+                                                                           const std::vector<double>& Y) {
+        const int n = int(rho.size());
+        if (deltaT.size() != size_t(n) || deltaTChem.size() != size_t(n) || Y.size() != size_t(n) * nEqns_)
+            throw std::invalid_argument("computeRR: array sizes");
+        std::vector<double> RR(size_t(n) * nSpecie_), dtc(n);
+        double minDeltaT = 0.0;
+        check(gf_compute_rr_lts(solver_, n, deltaT.data(), deltaTChemMax, rho.data(), deltaTChem.data(), Y.data(),
+                                RR.data(), dtc.data(), &minDeltaT));
+        return std::make_tuple(std::move(RR), std::move(dtc), minDeltaT);
+    }
+
     int nCells() const { return nCells_; }
     gf_solver* solver() { return solver_; }
     gf_mech* mechanism() { return mech_; }

@@ -157,6 +157,37 @@ def test_compute_rr_mirror(torch):
     assert (np.abs(RR.reshape(n, -1) - ref_RR) <= tol).all()
 
 
+def test_compute_rr_local_time_step(torch):
+    """computeRR with a flow step per cell (gf_compute_rr_lts, host arrays) against
+    gf_solve with deltaT_cell on device memory: the same kernel, bit for bit, and
+    RR = rho (Ynew - Y0) / deltaT_i with each cell's own step."""
+    g, raw, mech = gpu_mech("h2size")
+    cells = g["cells"]
+    n = cells.shape[0]
+    rng = np.random.default_rng(4)
+    dts = M.log_uniform(rng, 1e-7, 1e-5, n)
+    rho = np.linspace(0.3, 1.2, n)
+    dt0 = np.full(n, 1e-7)
+    ev = E.GpuKernelEvaluator(n, raw.n_eqns, raw.n_species, mech,
+                              E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4))
+    RR, dtn, mn = ev.computeRRLocal(dts, 5e-8, rho, dt0, cells)
+    s = E.Solver([mech], E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4))
+    s.set_launch(**ev.solver.get_launch())
+    Yd = torch.as_tensor(cells, device="cuda")
+    dtc = torch.as_tensor(dt0, device="cuda").clone()
+    out = s.solve(Yd, 0.0, dtc, deltaTChemMax=5e-8, rho=torch.as_tensor(rho, device="cuda"),
+                  deltaT_cell=torch.as_tensor(dts, device="cuda"), RR=torch.zeros((n, raw.n_species),
+                                                                              dtype=torch.float64, device="cuda"))
+    torch.cuda.synchronize()
+    assert np.array_equal(RR.reshape(n, -1), out["RR"].cpu().numpy())
+    assert np.array_equal(dtn, dtc.cpu().numpy()) and mn == out["stats"]["min_delta_t"]
+    Yn = out["Ynew"].cpu().numpy()
+    ref = rho[:, None] * (Yn[:, :raw.n_species] - cells[:, :raw.n_species]) / dts[:, None]
+    assert np.array_equal(RR.reshape(n, -1), ref)
+    with pytest.raises(ValueError):
+        ev.computeRRLocal(dts[:-1], 5e-8, rho, dt0, cells)
+
+
 def test_treact_gate(torch):
     g, raw, mech = gpu_mech("h2size")
     Treact = float(g["treact"])
