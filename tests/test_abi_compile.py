@@ -33,6 +33,13 @@ CXX_SRC = r"""
 #include <cstdio>
 #include <stdexcept>
 #include "gpufoam_b200.hpp"
+// both computeRR overloads compile (the per-cell one: local time stepping)
+double use_overloads(FoamGpu::GpuKernelEvaluator& ev) {
+    std::vector<double> rho{1.0}, dtc{1e-7}, Y(4, 0.0), dT{1e-6};
+    auto a = ev.computeRR(1e-6, 1.0, rho, dtc, Y);
+    auto b = ev.computeRR(dT, 1.0, rho, dtc, Y);
+    return std::get<2>(a) + std::get<2>(b);
+}
 int main() {
     int fails = 0;
     gf_ode_inputs in = FoamGpu::make_gf_ode_inputs("Rosenbrock23", 1e-8, 1e-4);
