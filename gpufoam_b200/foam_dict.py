@@ -1,4 +1,4 @@
-"""Reader of OpenFOAM chemistry dictionaries into a RawMechanism.
+"""Reader (and writer) of OpenFOAM chemistry dictionaries for a RawMechanism.
 
 The OpenFOAM side of the gpuFoam plugin builds its device mechanism from two
 dictionaries: the species thermo (``physicalProperties``/``thermo.compressibleGas``:
@@ -371,3 +371,91 @@ def read_mechanism_files(thermo_path: str, reactions_path: str, name: str = None
     with open(reactions_path) as f:
         rt = f.read()
     return read_mechanism(tt, rt, name or reactions_path)
+
+
+# --------------------------------------------------------------------------
+# writer: a RawMechanism as the two OpenFOAM dictionaries (the inverse of
+# read_mechanism), so that seeded synthetic mechanisms can be run by an
+# OpenFOAM + gpuFoam installation as they are run here
+
+_TYPE_NAMES = {RATE_THIRD_BODY: "reversibleThirdBodyArrhenius",
+               RATE_LINDEMANN: "reversibleArrheniusLindemannFallOff",
+               RATE_TROE: "reversibleArrheniusTroeFallOff"}
+
+
+def _num(x: float) -> str:
+    """A float that reads back bit for bit (repr), without an exponent when it
+    prefixes a species name."""
+    return repr(float(x))
+
+
+def _prefix(x: float) -> str:
+    s = repr(float(x))
+    if "e" in s or "E" in s or "inf" in s or "nan" in s:
+        raise ValueError(f"stoichiometric coefficient {x!r} cannot be written as a prefix")
+    return s[:-2] if s.endswith(".0") else s
+
+
+def _side(entries, species) -> str:
+    terms = []
+    for i, st, ex in entries:
+        t = ("" if st == 1.0 else _prefix(st)) + species[i]
+        if ex != st:
+            t += "^" + _num(ex)
+        terms.append(t)
+    return " + ".join(terms)
+
+
+def _efficiencies_text(eff, species, indent) -> str:
+    pad = " " * indent
+    pairs = "\n".join(f"{pad}    ({s} {_num(e)})" for s, e in zip(species, eff))
+    return f"{pad}coeffs {len(species)}\n{pad}(\n{pairs}\n{pad});\n"
+
+
+def write_mechanism(raw: RawMechanism):
+    """(thermo dictionary text, reactions dictionary text) of a RawMechanism."""
+    sp = raw.species
+    th = [f"species {len(sp)} ( {' '.join(sp)} );\n"]
+    for i, s in enumerate(sp):
+        th.append(
+            f"{s}\n{{\n    specie\n    {{\n        molWeight {_num(raw.W[i])};\n    }}\n"
+            f"    thermodynamics\n    {{\n        Tlow {_num(raw.Tlow[i])};\n        Thigh {_num(raw.Thigh[i])};\n"
+            f"        Tcommon {_num(raw.Tcommon[i])};\n"
+            f"        highCpCoeffs ( {' '.join(_num(c) for c in raw.high_raw[i])} );\n"
+            f"        lowCpCoeffs ( {' '.join(_num(c) for c in raw.low_raw[i])} );\n    }}\n}}\n")
+    rx = ["reactions\n{\n"]
+    for k, r in enumerate(raw.reactions):
+        eq = f"{_side(r.lhs, sp)} = {_side(r.rhs, sp)}"
+        body = []
+        if r.rate_type == RATE_ARRHENIUS:
+            body.append(f"type {'irreversibleArrhenius' if r.irreversible else 'reversibleArrhenius'};")
+        else:
+            if r.irreversible:
+                raise ValueError("the loader has no irreversible third-body or fall-off reaction type")
+            body.append(f"type {_TYPE_NAMES[r.rate_type]};")
+        body.append(f'reaction "{eq}";')
+        lines = "".join(f"        {b}\n" for b in body)
+        if r.rate_type in (RATE_ARRHENIUS, RATE_THIRD_BODY):
+            lines += f"        A {_num(r.A)};\n        beta {_num(r.beta)};\n        Ta {_num(r.Ta)};\n"
+            if r.rate_type == RATE_THIRD_BODY:
+                lines += _efficiencies_text(r.efficiencies, sp, 8)
+        else:
+            lines += (f"        k0\n        {{\n            A {_num(r.A)};\n            beta {_num(r.beta)};\n"
+                      f"            Ta {_num(r.Ta)};\n        }}\n"
+                      f"        kInf\n        {{\n            A {_num(r.Ainf)};\n            beta {_num(r.betainf)};\n"
+                      f"            Ta {_num(r.Tainf)};\n        }}\n")
+            if r.rate_type == RATE_TROE:
+                a, t3, t1, t2 = r.troe
+                lines += (f"        F\n        {{\n            alpha {_num(a)};\n            Tsss {_num(t3)};\n"
+                          f"            Ts {_num(t1)};\n            Tss {_num(t2)};\n        }}\n")
+            else:
+                lines += "        F\n        {\n        }\n"
+            lines += "        thirdBodyEfficiencies\n        {\n" + _efficiencies_text(r.efficiencies, sp, 12) + \
+                     "        }\n"
+        rx.append(f"    un-named-reaction-{k}\n    {{\n{lines}    }}\n")
+    rx.append("}\n")
+    if raw.rxn_Tlow != 0.0:
+        rx.append(f"Tlow {_num(raw.rxn_Tlow)};\n")
+    if raw.rxn_Thigh != DBL_MAX_OVER_10:
+        rx.append(f"Thigh {_num(raw.rxn_Thigh)};\n")
+    return "".join(th), "".join(rx)
