@@ -459,3 +459,32 @@ def write_mechanism(raw: RawMechanism):
     if raw.rxn_Thigh != DBL_MAX_OVER_10:
         rx.append(f"Thigh {_num(raw.rxn_Thigh)};\n")
     return "".join(th), "".join(rx)
+
+
+def main(argv=None) -> int:
+    """python -m gpufoam_b200.foam_dict MECHANISM SEED OUTDIR: writes the seeded
+    synthetic mechanism (h2_size, coverage, gri_size, large) as OUTDIR/thermo
+    and OUTDIR/reactions."""
+    import argparse
+    import os
+
+    from . import mechanism as M
+    ap = argparse.ArgumentParser(prog="python -m gpufoam_b200.foam_dict")
+    ap.add_argument("mechanism", choices=["h2_size", "coverage", "gri_size", "large"])
+    ap.add_argument("seed", type=int)
+    ap.add_argument("outdir")
+    args = ap.parse_args(argv)
+    raw = getattr(M, args.mechanism)(args.seed)
+    thermo, reactions = write_mechanism(raw)
+    os.makedirs(args.outdir, exist_ok=True)
+    with open(os.path.join(args.outdir, "thermo"), "w") as f:
+        f.write(thermo)
+    with open(os.path.join(args.outdir, "reactions"), "w") as f:
+        f.write(reactions)
+    print(f"{args.mechanism} seed {args.seed}: {raw.n_species} species, {raw.n_reactions} reactions -> "
+          f"{args.outdir}/thermo, {args.outdir}/reactions")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

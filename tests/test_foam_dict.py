@@ -164,3 +164,15 @@ def test_writer_rejects_what_the_loader_cannot_read():
     r.irreversible = True
     with pytest.raises(ValueError, match="irreversible"):
         F.write_mechanism(raw)
+
+
+def test_export_command(tmp_path):
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, "-m", "gpufoam_b200.foam_dict", "gri_size", "0", str(tmp_path)],
+                         cwd=ROOT, capture_output=True, text=True, check=True, timeout=120)
+    assert "53 species, 325 reactions" in out.stdout
+    back = F.read_mechanism_files(str(tmp_path / "thermo"), str(tmp_path / "reactions"))
+    raw = M.gri_size(0)
+    for k, v in flatten(raw).items():
+        assert np.array_equal(np.asarray(v), np.asarray(flatten(back)[k])), k
