@@ -171,6 +171,27 @@ def test_side_paths_port_vs_reference(name):
 
 
 @needs_ref
+@pytest.mark.parametrize("name", ["foam_h2", "foam_gri", "foam_yao"])
+def test_reference_test_configuration(name):
+    """The reference's own unit-test configuration: its real mechanisms at its test
+    condition (testHelpers/mechanisms.H:36-107, state 0 of the fixtures) with its
+    ODE inputs (absTol 1e-12, relTol 1e-1, create_gpu_inputs.C:59-71), every
+    Rosenbrock solver, over 1e-7 and 1e-5 s: the restatement equals the
+    reference bit for bit, step counts included."""
+    g = load(name)
+    mech = fixture_mech(g)
+    a, b = Oracle(mech, "port"), Oracle(mech, "reference")
+    cells = np.vstack([g["states"][:1], g["cells"][1:3]])
+    for s in (12, 23, 34):
+        inp = ode_inputs(s, absTol=1e-12, relTol=1e-1)
+        for dT in (1e-7, 1e-5):
+            ra = a.cells(inp, cells, dT, 1e-7)
+            rb = b.cells(inp, cells, dT, 1e-7)
+            for x, y in zip(ra[:3], rb[:3]):
+                assert eq(x, y)
+
+
+@needs_ref
 def test_reference_counted_wrapper_matches_reference_functor():
     """The counting wrapper used for step counts gives the same states as the
     reference's own singleCellSolver functor."""
