@@ -671,7 +671,9 @@ int solve_args(const gf_solver* s, int n_cells, double deltaT, const double* del
     if (ld_y < s->max_neq) return GF_ERR_INVALID_ARGUMENT;
     if (RR && (!rho || ld_rr < 1)) return GF_ERR_INVALID_ARGUMENT;
     if (!mech_id && s->mechs.size() > 1) return GF_ERR_INVALID_ARGUMENT;
-    if (RR && s->mechs.size() == 1 && ld_rr < s->dmechs[0].nS) return GF_ERR_INVALID_ARGUMENT;
+    if (RR)
+        for (const gf::DevMech& m : s->dmechs)
+            if (ld_rr < m.nS) return GF_ERR_INVALID_ARGUMENT;  // every cell's row must hold its species
     a->n_cells = n_cells;
     a->deltaT = deltaT;
     a->deltaT_cell = deltaT_cell;

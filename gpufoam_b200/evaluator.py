@@ -175,6 +175,18 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
+def _check_rows(Y0, Ynew, RR, n):
+    """The solve writes Ynew with Y0's row stride and RR with its own: both must
+    be row-contiguous 2-D tensors of n rows (RR at least as wide as the species)."""
+    for name, t in (("Y0", Y0), ("Ynew", Ynew), ("RR", RR)):
+        if t is None:
+            continue
+        if t.dim() != 2 or t.shape[0] != n or t.stride(1) != 1:
+            raise ValueError(f"{name} must be a row-contiguous [n_cells][k] tensor")
+    if Ynew is not None and (Ynew.shape[1] != Y0.shape[1] or Ynew.stride(0) != Y0.stride(0)):
+        raise ValueError("Ynew must have Y0's shape and row stride")
+
+
 class Solver:
     """gf_solver: one or more mechanisms + ODE inputs + Treact + launch form."""
 
@@ -208,17 +220,18 @@ class Solver:
         Returns dict(Ynew, RR, deltaTChem, status, counters, stats)."""
         import torch
         n = int(Y0.shape[0])
-        ld = int(Y0.shape[1])
+        ld = int(Y0.stride(0))
         if Ynew is None:
             Ynew = torch.empty_like(Y0)
         if rho is not None and RR is None:
             RR = torch.empty((n, ld), dtype=torch.float64, device=Y0.device)
         status = torch.empty(n, dtype=torch.int32, device=Y0.device) if want_status else None
         counters = torch.empty((n, 2), dtype=torch.int32, device=Y0.device) if want_counters else None
+        _check_rows(Y0, Ynew, RR, n)
         st = N.GfStats()
         N.check(self.lib.gf_solve(self.handle, n, float(deltaT), _ptr(deltaT_cell), float(deltaTChemMax),
                                   _ptr(mech_id), _ptr(rho), _ptr(Y0), ld, _ptr(Ynew), _ptr(deltaTChem), _ptr(RR),
-                                  ld if RR is not None else 0, _ptr(status), _ptr(counters),
+                                  int(RR.stride(0)) if RR is not None else 0, _ptr(status), _ptr(counters),
                                   C.byref(st) if want_stats else None, _stream_ptr(stream)), "gf_solve")
         return dict(Ynew=Ynew, RR=RR, deltaTChem=deltaTChem, status=status, counters=counters,
                     stats=dict(accepted=st.accepted_steps, attempts=st.attempts, failed=st.failed_cells,
@@ -230,16 +243,17 @@ class Solver:
         every launch re-reads Y0 / deltaTChem and rewrites Ynew, RR, status, counters in place."""
         import torch
         n = int(Y0.shape[0])
-        ld = int(Y0.shape[1])
+        ld = int(Y0.stride(0))
         if Ynew is None:
             Ynew = torch.empty_like(Y0)
         if rho is not None and RR is None:
             RR = torch.empty((n, ld), dtype=torch.float64, device=Y0.device)
+        _check_rows(Y0, Ynew, RR, n)
         h = C.c_void_p()
         N.check(self.lib.gf_solve_graph_create(self.handle, n, float(deltaT), _ptr(deltaT_cell), float(deltaTChemMax),
                                                _ptr(mech_id), _ptr(rho), _ptr(Y0), ld, _ptr(Ynew), _ptr(deltaTChem),
-                                               _ptr(RR), ld if RR is not None else 0, _ptr(status), _ptr(counters),
-                                               C.byref(h)), "gf_solve_graph_create")
+                                               _ptr(RR), int(RR.stride(0)) if RR is not None else 0, _ptr(status),
+                                               _ptr(counters), C.byref(h)), "gf_solve_graph_create")
         return SolveGraph(self, h, dict(Y0=Y0, deltaTChem=deltaTChem, rho=rho, deltaT_cell=deltaT_cell,
                                         mech_id=mech_id, Ynew=Ynew, RR=RR, status=status, counters=counters))
 

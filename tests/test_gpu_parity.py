@@ -176,8 +176,8 @@ def test_compute_rr_local_time_step(torch):
     Yd = torch.as_tensor(cells, device="cuda")
     dtc = torch.as_tensor(dt0, device="cuda").clone()
     out = s.solve(Yd, 0.0, dtc, deltaTChemMax=5e-8, rho=torch.as_tensor(rho, device="cuda"),
-                  deltaT_cell=torch.as_tensor(dts, device="cuda"), RR=torch.zeros((n, raw.n_species),
-                                                                              dtype=torch.float64, device="cuda"))
+                  deltaT_cell=torch.as_tensor(dts, device="cuda"),
+                  RR=torch.zeros((n, raw.n_species), dtype=torch.float64, device="cuda"))
     torch.cuda.synchronize()
     assert np.array_equal(RR.reshape(n, -1), out["RR"].cpu().numpy())
     assert np.array_equal(dtn, dtc.cpu().numpy()) and mn == out["stats"]["min_delta_t"]

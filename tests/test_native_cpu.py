@@ -107,3 +107,17 @@ def test_null_handles_rejected_without_a_device(lib):
     assert lib.gf_cell_rates(None, 4, None, None, 12, None, 10, None, None) == 1
     assert lib.gf_reaction_rates(None, 4, 0, None, None, 12, None, None, 10, None) == 1
     assert lib.gf_qdot(None, 4, None, 10, None, None) == 1
+
+
+def test_solve_row_checks():
+    """Solver.solve / capture refuse output tensors whose rows the kernel would
+    overrun (the row strides are passed to the C ABI as given)."""
+    import torch
+    Y0 = torch.zeros((4, 12), dtype=torch.float64)
+    E._check_rows(Y0, torch.zeros_like(Y0), torch.zeros((4, 10), dtype=torch.float64), 4)
+    with pytest.raises(ValueError):
+        E._check_rows(Y0, torch.zeros((4, 11), dtype=torch.float64), None, 4)
+    with pytest.raises(ValueError):
+        E._check_rows(Y0, None, torch.zeros((3, 10), dtype=torch.float64), 4)
+    with pytest.raises(ValueError):
+        E._check_rows(Y0, None, torch.zeros((10, 4), dtype=torch.float64).t(), 4)
