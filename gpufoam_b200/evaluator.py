@@ -382,10 +382,11 @@ def solve_noalloc(mech: Mechanism, ode: OdeInputs, Y0, deltaT: float, deltaTChem
     Returns the statistics dict when stats=True (this synchronises the stream)."""
     lib = N.load()
     n = int(Y0.shape[0])
+    _check_rows(Y0, Ynew, RR, n)
     st = N.GfStats()
     N.check(lib.gf_solve_noalloc(mech.handle, C.byref(ode.to_c()), float(Treact), n, float(deltaT), None,
-                                 float(deltaTChemMax), _ptr(rho), _ptr(Y0), int(Y0.shape[1]), _ptr(Ynew),
-                                 _ptr(deltaTChem), _ptr(RR), int(RR.shape[1]) if RR is not None else 0,
+                                 float(deltaTChemMax), _ptr(rho), _ptr(Y0), int(Y0.stride(0)), _ptr(Ynew),
+                                 _ptr(deltaTChem), _ptr(RR), int(RR.stride(0)) if RR is not None else 0,
                                  _ptr(status), _ptr(counters), C.byref(st) if stats else None, _stream_ptr(stream)),
             "gf_solve_noalloc")
     if stats:
@@ -482,6 +483,9 @@ def gather_states(Y_fields, T, p, ld: Optional[int] = None):
     nS = len(Y_fields)
     n = int(T.shape[0])
     ld = ld or nS + 2
+    for f in list(Y_fields) + [T, p]:
+        if f.dtype != torch.float64 or not f.is_cuda or not f.is_contiguous() or f.numel() < n:
+            raise ValueError("fields must be contiguous float64 cuda tensors of at least n cells")
     y = torch.zeros((n, ld), dtype=torch.float64, device="cuda")
     ptrs = (C.c_void_p * max(nS, 1))(*[f.data_ptr() for f in Y_fields])
     lib = N.load()
@@ -491,8 +495,14 @@ def gather_states(Y_fields, T, p, ld: Optional[int] = None):
 
 def scatter_rates(RR, RR_fields):
     """Cell-major rates RR [n][>= nS] -> the per-species fields RR_fields (nS cuda tensors of n)."""
+    import torch
     nS = len(RR_fields)
+    n = int(RR.shape[0])
+    if RR.dim() != 2 or RR.stride(1) != 1 or RR.shape[1] < nS or RR.dtype != torch.float64 or not RR.is_cuda:
+        raise ValueError("RR must be a row-contiguous float64 cuda tensor [n][>= nS]")
+    for f in RR_fields:
+        if f.dtype != torch.float64 or not f.is_cuda or not f.is_contiguous() or f.numel() < n:
+            raise ValueError("RR fields must be contiguous float64 cuda tensors of at least n cells")
     ptrs = (C.c_void_p * max(nS, 1))(*[f.data_ptr() for f in RR_fields])
     lib = N.load()
-    N.check(lib.gf_scatter_rates(int(RR.shape[0]), nS, _ptr(RR), int(RR.shape[1]), ptrs, _stream_ptr()),
-            "gf_scatter_rates")
+    N.check(lib.gf_scatter_rates(n, nS, _ptr(RR), int(RR.stride(0)), ptrs, _stream_ptr()), "gf_scatter_rates")
