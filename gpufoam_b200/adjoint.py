@@ -84,6 +84,8 @@ class AdjointSolver:
         Returns Ynew and keeps the recording for backward()."""
         import torch
         n, ld = Y0.shape
+        if deltaTChem.numel() != n or deltaTChem.dtype != torch.float64 or not deltaTChem.is_contiguous():
+            raise ValueError("deltaTChem must be a contiguous float64 tensor of one value per cell")
         lib = N.load()
         Y0 = Y0.contiguous()
         Ynew = torch.empty_like(Y0)
@@ -105,6 +107,8 @@ class AdjointSolver:
         rec = self._rec
         n, ld = rec["Y0"].shape
         lib = N.load()
+        if tuple(Ybar.shape) != (n, ld):
+            raise ValueError("Ybar must have the shape of the recorded states")
         Ybar = Ybar.contiguous().to(torch.float64)
         Y0bar = torch.zeros_like(rec["Y0"])
         thb = torch.zeros((n, self.raw.n_reactions * 3), dtype=torch.float64, device=Ybar.device)
