@@ -225,6 +225,20 @@ def test_determinism(torch):
         assert np.array_equal(first[0], again[0]) and np.array_equal(first[2], again[2])
 
 
+@pytest.mark.parametrize("launch", ["plain", "persist-g64-smem", "persist-g8-smem"])
+def test_all_cells_equal(torch, launch):
+    """The reference's single-cell-solver test shape (every cell the same state,
+    gpu_test_kernels.cu:659-749): every cell's result and step counts equal,
+    bit for bit, whichever slot or group integrated it."""
+    g, raw, mech = gpu_mech("foam_gri")
+    cells = np.repeat(g["states"][:1], 300, axis=0)
+    Y, dtc, cnt, st, _ = run_cells(torch, mech, cells, 1e-6, 1e-7, 34, LAUNCHES[launch])
+    assert (st == 0).all()
+    assert (Y == Y[0]).all() and (dtc == dtc[0]).all() and (cnt == cnt[0]).all()
+    ref = Oracle(raw, "port").cells(ode_inputs(34), cells[:1], 1e-6, 1e-7)
+    assert_states_close(Y[:1], ref[0], raw.n_species, 1e-4, launch)
+
+
 def test_mixed_mechanisms_per_cell_dt(torch):
     """One launch over cells of two mechanisms with per-cell deltaT and p."""
     raws = [M.h2_size(0), M.coverage(0)]
