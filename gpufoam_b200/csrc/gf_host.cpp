@@ -488,6 +488,31 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
         sexp.push_back(0.0);
     }
 
+    // ---- every index the kernels follow, checked before upload: a table that
+    // would send a kernel outside its arrays is refused here, not found on the GPU
+    {
+        const int m = nS + 1;
+        auto stream_ok = [](const std::vector<StreamRec>& rec, int n_pos, int n_src) {
+            for (const StreamRec& r : rec)
+                if (r.pos >= n_pos || r.slot >= n_src) return false;
+            return true;
+        };
+        const int n_conc_slots = 2 * kSideInline * nRa;
+        for (int k = 0; k < kNumGroupSizes; ++k)
+            if (!stream_ok(dst_rec[k], nS, n_slots) || !stream_ok(jst_rec[k], m * ldJ, n_slots) ||
+                !stream_ok(cst_rec[k], nS, n_conc_slots))
+                return GF_ERR_UNSUPPORTED;
+        for (int q = 0; q < nR; ++q) {
+            const int need = std::max(4, 2 + nl[q] + nr[q] + (rtype[q] == GF_RATE_THIRD_BODY_ARRHENIUS ? 1 : 0));
+            if (slot[q] < 0 || slot[q] + need > n_slots) return GF_ERR_UNSUPPORTED;
+            if (tb_row[q] >= n_tb || (rtype[q] != GF_RATE_ARRHENIUS && tb_row[q] < 0)) return GF_ERR_UNSUPPORTED;
+            if (sp_off[q] < 0 || (size_t)sp_off[q] + nl[q] + nr[q] > sidx.size()) return GF_ERR_UNSUPPORTED;
+            for (int e = 0; e < nl[q] + nr[q]; ++e)
+                if (sidx[sp_off[q] + e] < 0 || sidx[sp_off[q] + e] >= nS) return GF_ERR_UNSUPPORTED;
+        }
+        if (eff.size() < (size_t)std::max(n_tb, 1) * (n_tb > 0 ? nS : 1)) return GF_ERR_UNSUPPORTED;
+    }
+
     // ---- one device allocation
     DevBuf b;
     const size_t oW = b.add(W), oR = b.add(Rsp), oTc = b.add(Tc), oCoef = b.add(coef), oHf = b.add(hf);

@@ -121,3 +121,18 @@ def test_solve_row_checks():
         E._check_rows(Y0, None, torch.zeros((3, 10), dtype=torch.float64), 4)
     with pytest.raises(ValueError):
         E._check_rows(Y0, None, torch.zeros((10, 4), dtype=torch.float64).t(), 4)
+
+
+@pytest.mark.parametrize("name", ["h2size", "coverage", "grisize", "foam_h2", "foam_gri", "foam_yao"])
+def test_device_tables_pass_the_bounds_check(lib, name):
+    """gf_mech_create checks every index the kernels follow (gather-stream
+    positions and slots, staging slots, third-body rows, species entries) before
+    it allocates: on a machine without a GPU a valid mechanism gets as far as the
+    allocation (GF_ERR_NO_DEVICE), a bad table would stop at GF_ERR_UNSUPPORTED."""
+    import torch
+    from tests.test_oracle import fixture_mech
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the allocation succeeds")
+    raw = fixture_mech(dict(np.load(os.path.join(GOLDEN, f"{name}.npz"))))
+    with pytest.raises(N.GfError, match="GF_ERR_NO_DEVICE"):
+        E.Mechanism(raw)
