@@ -21,7 +21,7 @@ STATUS_NAMES = {
     4: "GF_ERR_MASS_IMBALANCE", 5: "GF_ERR_CUDA", 6: "GF_ERR_NO_DEVICE", 7: "GF_ERR_OUT_OF_MEMORY",
     8: "GF_ERR_CELL_FAILURE",
 }
-CELL_OK, CELL_STEP_UNDERFLOW, CELL_MAX_STEPS, CELL_NONFINITE, CELL_SKIPPED = range(5)
+CELL_OK, CELL_STEP_UNDERFLOW, CELL_MAX_STEPS, CELL_NONFINITE, CELL_SKIPPED, CELL_BAD_MECHANISM = range(6)
 
 # every symbol the header declares
 EXPORTS = [

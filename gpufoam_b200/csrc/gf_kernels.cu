@@ -26,9 +26,13 @@ __global__ void __launch_bounds__(128) plain_kernel(const MechSet P, const Launc
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= a.n_cells) return;
     Grp<1> g;
-    const DevMech& M = pick(P, a, cell);
+    const DevMech* M = pick(P, a, cell);
+    if (!M) {
+        reject_cell(a, cell);
+        return;
+    }
     WsS w{a.ws + cell, a.ws_slot_stride};
-    process_cell(g, M, w, a, (int)cell);
+    process_cell(g, *M, w, a, (int)cell);
 }
 
 __global__ void reset_kernel(unsigned long long* q) {
@@ -175,7 +179,7 @@ int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* 
 int launch_cells(const DevMech* mechs, int n_mechs, const gf_launch_config& cfg, const LaunchArgs& a,
                  int ws_doubles_per_cell, int n_slots_total, void* stream) {
     MechSet P;
-    P.n = n_mechs;
+    P.n = std::min(n_mechs, kMaxMechs);
     for (int i = 0; i < n_mechs && i < kMaxMechs; ++i) P.m[i] = mechs[i];
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     reset_kernel<<<1, 1, 0, s>>>(a.queue);

@@ -23,9 +23,16 @@ struct MechSet {
     int n;
 };
 
-__device__ __forceinline__ const DevMech& pick(const MechSet& P, const LaunchArgs& a, long long cell) {
+// The cell's mechanism, or null for an id outside the solver's mechanisms: the
+// cell is then not integrated, its status says so, and it counts as failed.
+__device__ __forceinline__ const DevMech* pick(const MechSet& P, const LaunchArgs& a, long long cell) {
     const int id = a.mech_id ? a.mech_id[cell] : 0;
-    return P.m[id];
+    return (id >= 0 && id < P.n) ? &P.m[id] : nullptr;
+}
+
+__device__ __forceinline__ void reject_cell(const LaunchArgs& a, long long cell) {
+    if (a.status) a.status[cell] = GF_CELL_BAD_MECHANISM;
+    atomicAdd(a.queue + 4, 1ull);
 }
 
 // threads per CTA the kernel is compiled for
@@ -49,7 +56,12 @@ __global__ void __launch_bounds__(PersistShape<G>::kThreads, SLIM ? PersistShape
         if (g.lane == 0) cell = (long long)atomicAdd(a.queue, 1ull);
         cell = g.bcast_ll(cell, 0);
         if (cell >= a.n_cells) break;
-        const DevMech& M = pick(P, a, cell);
+        const DevMech* Mp = pick(P, a, cell);
+        if (!Mp) {
+            if (g.lane == 0) reject_cell(a, cell);
+            continue;
+        }
+        const DevMech& M = *Mp;
         if (SHARED) {
             process_cell(g, M, WsC{smem + (size_t)gib * ws_per_cell}, a, (int)cell);
         } else if (G == 1) {

@@ -66,7 +66,8 @@ enum gf_cell_status {
     GF_CELL_STEP_UNDERFLOW = 1,   /* dx < vSmall during step rejection           */
     GF_CELL_MAX_STEPS = 2,        /* maxSteps substeps taken before reaching deltaT */
     GF_CELL_NONFINITE = 3,        /* NaN/Inf in the integrated state             */
-    GF_CELL_SKIPPED = 4           /* T <= Treact: chemistry not solved (not an error) */
+    GF_CELL_SKIPPED = 4,          /* T <= Treact: chemistry not solved (not an error) */
+    GF_CELL_BAD_MECHANISM = 5     /* mech_id outside the solver's mechanisms: not integrated */
 };
 
 /* Reaction-rate kinds (gpuReactionRate variant, gpuReactionRate.H:16-28). */
@@ -195,7 +196,8 @@ int gf_solver_get_launch(const gf_solver* solver, gf_launch_config* cfg);
  *   deltaT         flow time step (used when deltaT_cell is NULL)
  *   deltaT_cell    per-cell time step [n_cells] or NULL (local time stepping)
  *   deltaTChemMax  clamp for the returned chemistry time steps
- *   mech_id        per-cell mechanism index [n_cells] or NULL (all mechanism 0)
+ *   mech_id        per-cell mechanism index [n_cells] or NULL (all mechanism 0); a cell whose
+ *                  id is outside 0 .. n_mechs-1 is not integrated (GF_CELL_BAD_MECHANISM)
  *   rho            old-time density [n_cells] (may be NULL when RR is NULL)
  *   Y0             input states [n_cells][nEqns of the cell's mechanism], row stride ld_y
  *   Ynew           output states, same layout (may alias Y0, may be NULL)
