@@ -2,7 +2,7 @@
 """Benchmark: cells/s per flow step (ΔT) of the per-cell chemistry solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload gri-100k|gri-bimodal-1M|h2-1k|mixed-750k] [--solver 34]
+                    [--workload gri-bimodal-1M|gri-100k|h2-1k|mixed-750k|...] [--solver 34]
                     [--no-plain] [--no-e2e] [--no-cpu]
 
 A step is one gf_solve over the whole batch: every cell integrated over one
@@ -12,17 +12,25 @@ reference tutorials' initialChemicalTimeStep). Inputs are seeded synthetic
 batches; L2 (126 MB) is flushed before every timed step by writing a 256 MB
 buffer (outside the timed region).
 
+The default workload is the 1M-cell batch of the 53-species mechanism with
+bimodal temperatures (40 % near-inert cells at 300-700 K, 60 % igniting cells
+at 1100-2400 K, shuffled): the batch the persistent-vs-plain comparison is
+stated on. Both arms print the same `metric` string.
+
 `value`     persistent work-queue kernel, captured once as a CUDA graph and
             replayed every step; inputs resident in HBM, CUDA events
 `plain`     the one-thread-per-cell kernel on the same batch (the reference's
             launch model, also replayed from a graph), for the
-            persistent-vs-plain ratio
+            persistent-vs-plain ratio; one untimed warm-up solve on a 64k-cell
+            part of the batch, then --plain-steps timed steps over all of it
+`substeps_per_cell` the spread of accepted substeps per cell over the batch
 `e2e`       GpuKernelEvaluator.computeRR through the C ABI from pinned host
             arrays: H2D of Y/ΔTChem/rho, the solve, D2H of RR/ΔTChem
 `roofline`  FP64 pipe: algorithmic FLOP (gpufoam_b200/flops.py) per launch ÷
             launch time, against the DFMA peak measured live on this GPU
 `cpu_baseline` the reference's own FP64 code (compiled in place, OpenMP over
-            cells on all host cores) on a bounded sample of the same batch
+            cells, one cell per scheduling chunk, on all host cores) on a
+            bounded sample of the same batch
 
 Multi-GPU (torchrun): every rank integrates its own batch of the workload's
 size (weak scaling, cells are independent); the one exchange per step is the
@@ -48,7 +56,10 @@ WORKLOADS = {
     # name: mechanism, cells, deltaT, T sampling
     "h2-1k": dict(mech="h2", n=1024, dT=1e-5, T=(1000.0, 2500.0)),
     "gri-100k": dict(mech="gri", n=100_000, dT=1e-6, T=(1000.0, 2500.0)),
-    "gri-bimodal-1M": dict(mech="gri", n=1_000_000, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0))),
+    # bimodal: 40 % near-inert cells (reactive mass fraction 1e-4, the rest the
+    # inert species) at 300-700 K and 60 % igniting cells at 1100-2400 K
+    "gri-bimodal-1M": dict(mech="gri", n=1_000_000, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0)),
+                           cold_reactive=1e-4),
     # one launch over three mechanisms (10, 53 and 100 species), per-cell
     # deltaT ~ log-U[1e-7, 1e-4] s and p ~ U[0.5, 40] atm, cells shuffled
     "mixed-750k": dict(mixed=((("h2", 200_000), ("gri", 500_000), ("large", 50_000))), dT=0.0,
@@ -59,12 +70,20 @@ WORKLOADS = {
     # small cases of the same kernels, for ncu captures and launch sweeps
     "gri-4k": dict(mech="gri", n=4096, dT=1e-6, T=(1000.0, 2500.0)),
     "gri-16k": dict(mech="gri", n=16384, dT=1e-6, T=(1000.0, 2500.0)),
-    "gri-bimodal-64k": dict(mech="gri", n=65536, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0))),
+    "gri-bimodal-64k": dict(mech="gri", n=65536, dT=1e-6, bimodal=(0.4, (300.0, 700.0), (1100.0, 2400.0)),
+                            cold_reactive=1e-4),
     # the real GRI-Mech 3.0 of the reference's unit tests (53 species, 325
     # reactions, read from its OpenFOAM dictionaries into tests/golden/foam_gri.npz)
     "gri30-100k": dict(mech="gri30", n=100_000, dT=1e-6, T=(1000.0, 2500.0)),
 }
 DTC0 = 1e-7
+
+
+def metric_name(workload, solver):
+    """The metric string both arms print (the driver pairs the lines by it)."""
+    return f"cells/s per ΔT at relTol 1e-4 ({workload}, R{solver})"
+
+
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of the
 # persistent kernel on the GRI-size mechanism, from one ncu capture of 4 096
 # cells (threads_per_cell 64, shared-memory workspace): 2 481 152 B read, 0 B
@@ -79,7 +98,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="gri-100k", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="gri-bimodal-1M", choices=list(WORKLOADS))
     ap.add_argument("--solver", type=int, default=34, choices=[12, 23, 34])
     ap.add_argument("--launch", default="auto", choices=["fixed", "auto", "sweep"],
                     help="fixed: --threads-per-cell/--shared; auto: autotuner on a sample; "
@@ -89,9 +108,10 @@ def parse():
     ap.add_argument("--register-budget", type=int, default=0, choices=[0, 1],
                     help="persistent kernel: 0 = up to 255 registers per thread, 1 = at most 128")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--plain-steps", type=int, default=2,
-                    help="timed steps of the plain-kernel leg (at most --steps; one warm-up step before). "
-                         "The plain kernel runs ~10x longer than the persistent one on mixed batches")
+    ap.add_argument("--plain-steps", type=int, default=1,
+                    help="timed steps of the plain-kernel leg over the whole batch (at most --steps), after "
+                         "one untimed warm-up solve on a 64k-cell part of it; the plain kernel runs several "
+                         "times longer than the persistent one on the bimodal and mixed batches")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -138,7 +158,8 @@ def make_batch(wl, seed) -> Batch:
         return Batch(raws, np.ascontiguousarray(cells[perm]), mid[perm], dts)
     raw = _mech(wl["mech"])
     if "bimodal" in wl:
-        cells = M.make_cells(raw, wl["n"], seed=seed, bimodal=wl["bimodal"])
+        cells = M.make_cells(raw, wl["n"], seed=seed, bimodal=wl["bimodal"],
+                             cold_reactive_fraction=wl.get("cold_reactive"))
     else:
         cells = M.make_cells(raw, wl["n"], seed=seed, T_range=wl["T"])
     return Batch([raw], cells)
@@ -186,31 +207,41 @@ class Clocks:
 
 
 def _cpu_rate_one(raw, cells, solver, dT, dT_cell, seconds, nthreads):
+    """cells/s of the CPU path on one mechanism: a short call sizes the sample,
+    then one call over about `seconds` of cells (at least 32 per thread), each
+    cell its own OpenMP scheduling chunk so every thread stays busy to the end.
+    Returns (cells/s of the sized call, cells in it, kind, its seconds)."""
     from oracle.oracle import REF_LIB, Oracle, ode_inputs
     kind = "reference" if os.path.exists(REF_LIB) else "port"
     o = Oracle(raw, kind)
     inp = ode_inputs(solver)
-    n = max(nthreads * 4, 32)
-    done, t_total = 0, 0.0
-    while t_total < seconds and done < cells.shape[0]:
-        chunk = np.ascontiguousarray(cells[done:done + n, :raw.n_eqns])
+
+    def run(lo, hi):
+        chunk = np.ascontiguousarray(cells[lo:hi, :raw.n_eqns])
         t0 = time.perf_counter()
         if kind == "reference" and dT_cell is None:
             o.cells_uncounted(inp, chunk, dT, DTC0, nthreads=nthreads)
         else:
-            o.cells(inp, chunk, dT, DTC0, deltaT_cell=None if dT_cell is None else dT_cell[done:done + n],
+            o.cells(inp, chunk, dT, DTC0, deltaT_cell=None if dT_cell is None else dT_cell[lo:hi],
                     nthreads=nthreads)
-        t_total += time.perf_counter() - t0
-        done += chunk.shape[0]
-        n = min(n * 2, 4096)
-    return done / t_total, done, kind, t_total
+        return time.perf_counter() - t0
+
+    n_all = cells.shape[0]
+    probe = min(n_all, 4 * nthreads)
+    rate = probe / max(run(0, probe), 1e-9)
+    size = int(min(n_all - probe, max(32 * nthreads, rate * seconds)))
+    if size <= 0:
+        return rate, probe, kind, probe / rate
+    t = run(probe, probe + size)
+    return size / t, size, kind, t
 
 
 def cpu_reference_rate(batch, solver, dT, seconds, nthreads, offset=0):
     """The reference's own singleCellSolver (oracle/_ref, or the port) over a
-    bounded sample of the batch with all host threads. Several mechanisms: each
-    is timed on its own cells for a share of the time, and the batch rate is
-    n / sum_k(n_k / rate_k). Returns (cells/s, sample size, kind, seconds)."""
+    bounded sample of the batch (from `offset`; the batches are shuffled) with
+    all host threads. Several mechanisms: each is timed on its own cells for a
+    share of the time, and the batch rate is n / sum_k(n_k / rate_k).
+    Returns (cells/s, sample size, kind, seconds)."""
     if batch.mech_id is None:
         return _cpu_rate_one(batch.raws[0], batch.cells[offset:], solver, dT, None, seconds, nthreads)
     n = batch.cells.shape[0]
@@ -275,6 +306,7 @@ def adjoint_measure(solver_launch, steps, n_cells=4096):
     f, r, a = float(np.mean(fw)), float(np.mean(rec)), float(np.mean(adj))
     return {"workload": f"{n_cells} GRI-size cells, T~U[1100,1600] K, deltaT 1e-4 s, Rosenbrock34",
             "forward_ms": f, "forward_recording_ms": r, "adjoint_ms": a, "adjoint_over_forward": a / f,
+            "gradient_over_forward": (r + a) / f,
             "accepted_steps_per_cell": {"mean": float(cnt[:, 0].mean()), "max": int(cnt[:, 0].max())},
             "cells_ok": ok, "parameters": f"{raw.n_reactions} x (ln|A|, beta, Ta)"}
 
@@ -302,22 +334,24 @@ def main():
             return
         batch = make_batch(wl, seed=1000)
         times, rates, sample = [], [], None
+        n_all = batch.cells.shape[0]
         for k in range(args.warmup + args.steps):
             r, done, kind, t = cpu_reference_rate(batch, args.solver, wl["dT"], max(2.0, args.cpu_seconds / 4),
-                                                  nthreads, offset=(k * 997) % max(1, batch.cells.shape[0] - 4096))
+                                                  nthreads, offset=(k * 7919 * nthreads) % max(1, n_all // 2))
             if k >= args.warmup:
                 rates.append(r)
                 times.append(t)
                 sample = done
         value = float(np.mean(rates))
-        line = {"impl": "reference", "metric": f"cells/s per ΔT at relTol 1e-4 ({args.workload}, R{args.solver})",
+        line = {"impl": "reference", "metric": metric_name(args.workload, args.solver),
                 "value": value, "unit": "cells/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": dict(cfg_desc, cells=int(batch.cells.shape[0])),
                 "cpu_baseline": {"value": value, "unit": "cells/s", "cores": nthreads, "kind": kind,
-                                 "sample": f"{sample} cells of the {args.workload} batch per step, OpenMP "
-                                           f"schedule(dynamic,64) over cells"},
+                                 "sample": f"{sample} cells of the {args.workload} batch per step (a new "
+                                           f"part of the shuffled batch each step), the reference's "
+                                           f"singleCellSolver per cell, OpenMP schedule(dynamic,1) over cells"},
                 "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -428,14 +462,22 @@ def main():
     if not args.no_plain:
         ps = E.Solver(mechs, ode)
         ps.set_launch(kind=0)
-        pms, pcnt, _ = timed(ps, max(1, min(args.steps, args.plain_steps)), 1)
+        # warm-up: one untimed solve over a part of the batch (a plain step over
+        # the whole bimodal or mixed batch takes minutes)
+        k = min(n, 65536)
+        ps.solve(Y0[:k], wl["dT"], dtc0[:k].clone(), deltaT_cell=None if dtcell is None else dtcell[:k],
+                 mech_id=None if mid is None else mid[:k], want_status=False, want_counters=False,
+                 want_stats=False)
+        torch.cuda.synchronize()
+        pms, pcnt, _ = timed(ps, max(1, min(args.steps, args.plain_steps)), 0)
         pm = float(np.mean(pms))
         if world > 1:
             t = torch.tensor([pm], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             pm = float(t.item())
         plain = {"value": world * n / (pm * 1e-3), "ms_per_step": pm, "unit": "cells/s",
-                 "launch": "one thread per cell, HBM scratch"}
+                 "steps": len(pms), "launch": "one thread per cell, HBM scratch (the reference's launch model)",
+                 "warmup": f"one untimed solve over {k} cells of the batch"}
         del ps
 
     e2e = None
@@ -512,17 +554,26 @@ def main():
         r, done, kind, t = cpu_reference_rate(batch, args.solver, wl["dT"], args.cpu_seconds, nthreads)
         cpu = {"value": r, "unit": "cells/s", "cores": nthreads, "kind": kind,
                "sample": f"{done} cells of the {args.workload} batch ({t:.1f} s), the reference's "
-                         f"singleCellSolver per cell, OpenMP schedule(dynamic,64)"}
+                         f"singleCellSolver per cell, OpenMP schedule(dynamic,1)"}
+
+    acc = cnt[:, 0]
+    if batch.mech_id is not None:
+        acc = acc[acc > 0] if (acc > 0).any() else acc
+    spread = {"min": int(acc.min()), "p1": float(np.percentile(acc, 1)), "p50": float(np.percentile(acc, 50)),
+              "p99": float(np.percentile(acc, 99)), "max": int(acc.max()),
+              "max_over_min": float(acc.max() / max(acc.min(), 1)),
+              "p99_over_p1": float(np.percentile(acc, 99) / max(np.percentile(acc, 1), 1.0))}
 
     if rank == 0:
         line = {
-            "metric": f"cells/s per ΔT at relTol 1e-4 ({args.workload}, R{args.solver}, persistent kernel)",
+            "metric": metric_name(args.workload, args.solver),
             "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": dict(cfg_desc, cells_per_gpu=n,
                            mechanisms=[f"{r.n_species} species / {r.n_reactions} reactions" for r in batch.raws],
-                           deltaTChem0=DTC0, launch=solver.get_launch(), l2="flushed before each timed step (256 MB write)",
+                           deltaTChem0=DTC0, kernel="persistent work queue, CUDA-graph replay",
+                           launch=solver.get_launch(), l2="flushed before each timed step (256 MB write)",
                            parallelism=f"cells sharded over {world} GPU(s)"),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value,
@@ -535,6 +586,7 @@ def main():
                          "algorithmic_flop_per_launch": flop, "attempts": attempts, "accepted": accepted},
             "plain": plain,
             "persistent_vs_plain": (value / plain["value"]) if plain else None,
+            "substeps_per_cell": spread,
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
             "adjoint": adjoint,
         }

@@ -32,6 +32,7 @@ EXPORTS = [
     "gf_solve_record", "gf_adjoint", "gf_solve_graph_create", "gf_solve_graph_set_delta_t",
     "gf_solve_graph_launch", "gf_solve_graph_stats", "gf_solve_graph_destroy", "gf_cell_rates",
     "gf_reaction_rates", "gf_qdot", "gf_gather_states", "gf_scatter_rates", "gf_compute_rr_lts",
+    "gf_lu_factor_solve",
 ]
 
 
@@ -127,6 +128,7 @@ def load() -> C.CDLL:
     lib.gf_jacobian.argtypes = [vp, ip, vp, vp, vp, vp]
     lib.gf_lu_decompose.argtypes = [ip, ip, vp, vp, vp]
     lib.gf_lu_backsubstitute.argtypes = [ip, ip, vp, vp, vp, vp]
+    lib.gf_lu_factor_solve.argtypes = [ip, ip, vp, vp, vp, ip, ip, ip, vp]
     lib.gf_measure_fp64_peak.argtypes = [dp, P(dp)]
     lib.gf_solve_noalloc.argtypes = [vp, P(GfOdeInputs), dp, ip, dp, vp, dp, vp, vp, ip, vp, vp, vp, ip, vp, vp,
                                      P(GfStats), vp]

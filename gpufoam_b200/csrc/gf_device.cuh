@@ -911,12 +911,25 @@ __device__ __forceinline__ void row_scale(const Grp<G>& g, const W& w, int A, in
     g.sync();
 }
 
+// One elimination update a - l * u. The solve kernels contract it to one FMA
+// (EXACT = false); EXACT = true rounds the product and the difference
+// separately, as the reference's CPU build (no contraction) computes the Crout
+// sums of ludecompose.H:36-55, so that parity kernels can compare factors bit
+// for bit.
+template <bool EXACT>
+__device__ __forceinline__ double msub(double a, double l, double u) {
+    if constexpr (EXACT)
+        return __dsub_rn(a, __dmul_rn(l, u));
+    else
+        return fma(-l, u, a);
+}
+
 // LUDecompose (ludecompose.H:9-92) in right-looking form: at step k the pivot
 // column holds exactly the Crout sums of the reference, the pivot is the last
 // row with the largest vv*|a| (">=", :62), full rows are swapped, a zero pivot
 // becomes gpuSmall and the column below is scaled by 1/pivot. Every entry
 // receives its updates in the same k order as the reference's Crout loops.
-template <int G, class W>
+template <int G, bool EXACT = false, class W>
 __device__ __forceinline__ void lu_decompose(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv, int m) {
     for (int k = 0; k < m; ++k) {
         // pivot search
@@ -959,7 +972,7 @@ __device__ __forceinline__ void lu_decompose(const Grp<G>& g, const W& w, int A,
             g.sync();
             for (int j = k + 1 + g.lane; j < m; j += G) {
                 const double ukj = w[A + k * ld + j];
-                for (int i = k + 1; i < m; ++i) w[A + i * ld + j] -= w[A + i * ld + k] * ukj;
+                for (int i = k + 1; i < m; ++i) w[A + i * ld + j] = msub<EXACT>(w[A + i * ld + j], w[A + i * ld + k], ukj);
             }
             g.sync();
         }
@@ -974,7 +987,7 @@ __device__ __forceinline__ void lu_decompose(const Grp<G>& g, const W& w, int A,
 // Panel steps k0 .. k1-1 of the blocked LU (a group of at most one warp):
 // pivot search, row exchange, zero-pivot fix, column scaling and the update of
 // the panel's remaining columns.
-template <int G, class W>
+template <int G, bool EXACT = false, class W>
 __device__ __forceinline__ void lu_panel(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv, int m, int k0,
                                          int k1) {
     for (int k = k0; k < k1; ++k) {
@@ -1016,7 +1029,7 @@ __device__ __forceinline__ void lu_panel(const Grp<G>& g, const W& w, int A, int
             for (int i = k + 1 + g.lane; i < m; i += G) {
                 const double lik = w[A + i * ld + k] * rDiag;
                 w[A + i * ld + k] = lik;
-                for (int j = k + 1; j < k1; ++j) w[A + i * ld + j] -= lik * w[A + k * ld + j];
+                for (int j = k + 1; j < k1; ++j) w[A + i * ld + j] = msub<EXACT>(w[A + i * ld + j], lik, w[A + k * ld + j]);
             }
             g.sync();
         }
@@ -1038,7 +1051,7 @@ __device__ __forceinline__ void lu_panel(const Grp<G>& g, const W& w, int A, int
 // piv[]; the exchanges of the columns outside the panel are left to
 // lu_apply_swaps. Difference: when every candidate of a column is NaN, the
 // reference exchanges row k with row 0 (its iMax starts at 0); here none is.
-template <int RP, int NB, class W>
+template <int RP, int NB, bool EXACT = false, class W>
 __device__ __forceinline__ void lu_panel_reg(const Grp<32>& g, const W& w, int A, int ld, int piv, int vv, int m,
                                              int k0, int k1) {
     const int l = g.lane;
@@ -1123,7 +1136,7 @@ __device__ __forceinline__ void lu_panel_reg(const Grp<32>& g, const W& w, int A
                     a[r][kk] = lik;
 #pragma unroll
                     for (int t = kk + 1; t < NB; ++t)
-                        if (t < kb) a[r][t] -= lik * urow[t];
+                        if (t < kb) a[r][t] = msub<EXACT>(a[r][t], lik, urow[t]);
                 }
             }
         }
@@ -1158,7 +1171,7 @@ __device__ __forceinline__ void lu_apply_swaps(const W& w, int A, int ld, int pi
 // panel takes the panel's row exchanges, then (columns right of the panel) its
 // U12 rows; then the trailing matrix is updated (lanes over columns, warps over
 // rows). Every entry receives its updates in k order, as in lu_decompose.
-template <int G, int NB, class W>
+template <int G, int NB, bool EXACT = false, class W>
 __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv,
                                                       int m) {
     constexpr int NWp = G > 32 ? G / 32 : 1;
@@ -1171,7 +1184,7 @@ __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& 
             GF_PH_BEGIN(g)
             if (wid == 0) {
                 Grp<32> g32;
-                lu_panel_reg<2, NB>(g32, w, A, ld, piv, vv, m, k0, k1);
+                lu_panel_reg<2, NB, EXACT>(g32, w, A, ld, piv, vv, m, k0, k1);
             }
             g.sync();
             GF_PH_END(g, PH_LU_PANEL)
@@ -1191,7 +1204,7 @@ __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& 
                         if (t < kb) {
                             double v = u[t];
 #pragma unroll
-                            for (int t2 = 0; t2 < t; ++t2) v -= w[A + (k0 + t) * ld + k0 + t2] * u[t2];
+                            for (int t2 = 0; t2 < t; ++t2) v = msub<EXACT>(v, w[A + (k0 + t) * ld + k0 + t2], u[t2]);
                             u[t] = v;
                             w[A + (k0 + t) * ld + jj] = v;
                         }
@@ -1212,7 +1225,7 @@ __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& 
                     double a = w[A + i * ld + j];
 #pragma unroll
                     for (int t = 0; t < NB; ++t)
-                        if (t < kb) a -= w[A + i * ld + k0 + t] * u[t];
+                        if (t < kb) a = msub<EXACT>(a, w[A + i * ld + k0 + t], u[t]);
                     w[A + i * ld + j] = a;
                 }
             }
@@ -1223,7 +1236,7 @@ __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& 
     }
 }
 
-template <int G, int NB, class W>
+template <int G, int NB, bool EXACT = false, class W>
 __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv,
                                                      int m) {
     if constexpr (G > 32) {
@@ -1237,14 +1250,15 @@ __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w
             const int k1 = k0 + kb;
             if (wid == 0) {
                 Grp<32> g32;
-                lu_panel(g32, w, A, ld, piv, vv, m, k0, k1);
+                lu_panel<32, EXACT>(g32, w, A, ld, piv, vv, m, k0, k1);
             }
             __syncthreads();
             if (k1 >= m) break;
             for (int j = k1 + g.lane; j < m; j += G) {
                 for (int t = 1; t < kb; ++t) {
                     double v = w[A + (k0 + t) * ld + j];
-                    for (int t2 = 0; t2 < t; ++t2) v -= w[A + (k0 + t) * ld + k0 + t2] * w[A + (k0 + t2) * ld + j];
+                    for (int t2 = 0; t2 < t; ++t2)
+                        v = msub<EXACT>(v, w[A + (k0 + t) * ld + k0 + t2], w[A + (k0 + t2) * ld + j]);
                     w[A + (k0 + t) * ld + j] = v;
                 }
             }
@@ -1257,7 +1271,7 @@ __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w
                     double a = w[A + i * ld + j];
 #pragma unroll
                     for (int t = 0; t < NB; ++t)
-                        if (t < kb) a -= w[A + i * ld + k0 + t] * u[t];
+                        if (t < kb) a = msub<EXACT>(a, w[A + i * ld + k0 + t], u[t]);
                     w[A + i * ld + j] = a;
                 }
             }
@@ -1268,7 +1282,7 @@ __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w
         const int kb = min(NB, m - k0);
         const int k1 = k0 + kb;
         // 1. panel: columns [k0, k1), rows [k0, m)
-        lu_panel(g, w, A, ld, piv, vv, m, k0, k1);
+        lu_panel<G, EXACT>(g, w, A, ld, piv, vv, m, k0, k1);
         if (k1 >= m) break;
         // 2. U12: rows [k0, k1), columns [k1, m)
         for (int j = k1 + g.lane; j < m; j += G) {
@@ -1277,7 +1291,7 @@ __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w
             for (int t = 0; t < NB; ++t) {
                 if (t < kb) {
                     double v = w[A + (k0 + t) * ld + j];
-                    for (int t2 = 0; t2 < t; ++t2) v -= w[A + (k0 + t) * ld + k0 + t2] * u[t2];
+                    for (int t2 = 0; t2 < t; ++t2) v = msub<EXACT>(v, w[A + (k0 + t) * ld + k0 + t2], u[t2]);
                     u[t] = v;
                     w[A + (k0 + t) * ld + j] = v;
                 }
@@ -1287,7 +1301,7 @@ __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w
                 double a = w[A + i * ld + j];
 #pragma unroll
                 for (int t = 0; t < NB; ++t)
-                    if (t < kb) a -= w[A + i * ld + k0 + t] * u[t];
+                    if (t < kb) a = msub<EXACT>(a, w[A + i * ld + k0 + t], u[t]);
                 w[A + i * ld + j] = a;
             }
         }
@@ -1488,6 +1502,32 @@ __device__ __forceinline__ void lu_solve_any(const Grp<G>& g, const W& w, int A,
     lu_solve(g, w, A, ld, piv, m, b);
 }
 
+// The factorisation as the solve kernels run it, after the row scaling vv:
+// the register-panel form for a full warp or a multi-warp group (m <= 64),
+// the blocked form otherwise; then, for groups of 16 or more threads, the
+// reciprocal pivots 1 / U[i][i] (written over vv, which is no longer needed)
+// and the row permutation of the solves (lu_solve_any).
+template <int G, bool EXACT = false, class W>
+__device__ __forceinline__ void lu_factor(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv, int perm,
+                                          int m) {
+    {
+        GF_PH_BEGIN(g)
+        bool done = false;
+        if constexpr (G >= 32) {
+            if (m <= 64) {
+                lu_decompose_regpanel<G, 8, EXACT>(g, w, A, ld, piv, vv, m);
+                done = true;
+            }
+        }
+        if (!done) lu_decompose_blocked<G, 8, EXACT>(g, w, A, ld, piv, vv, m);
+        GF_PH_END(g, PH_LU)
+    }
+    if (G >= 16) {
+        for (int i = g.lane; i < m; i += G) w[vv + i] = 1.0 / w[A + i * ld + i];
+        lu_perm(g, w, piv, perm, m);
+    }
+}
+
 // ------------------------------------------------------------- Rosenbrock
 
 struct RosCoeffs {
@@ -1581,23 +1621,7 @@ __device__ __forceinline__ void shift_and_factor(const Grp<G>& g, const DevMech&
         shift_and_scale(g, w, L.J, ld, L.vv, m, 1.0 / (C.gamma * dx));
         GF_PH_END(g, PH_SHIFT)
     }
-    {
-        GF_PH_BEGIN(g)
-        bool done = false;
-        if constexpr (G >= 32) {
-            if (m <= 64) {
-                lu_decompose_regpanel<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
-                done = true;
-            }
-        }
-        if (!done) lu_decompose_blocked<G, 8>(g, w, L.J, ld, L.piv, L.vv, m);
-        GF_PH_END(g, PH_LU)
-    }
-    if (G >= 16) {
-        // the row scaling vv is no longer needed: it holds 1 / U[i][i] from here
-        for (int i = g.lane; i < m; i += G) w[L.vv + i] = 1.0 / w[L.J + i * ld + i];
-        lu_perm(g, w, L.piv, L.perm, m);
-    }
+    lu_factor(g, w, L.J, ld, L.piv, L.vv, L.perm, m);
 }
 
 // The Jacobian at y0, then shift_and_factor.

@@ -180,6 +180,8 @@ struct gf_solver {
 
 namespace gf {
 const DevMech* mech_device_tables(const gf_mech* m) { return &m->dev; }
+int mech_device(const gf_mech* m) { return m->device; }
+int record_cuda_error(int e) { return cuda_fail((cudaError_t)e); }
 }  // namespace gf
 
 namespace {
@@ -1103,6 +1105,17 @@ int gf_jacobian(const gf_mech* m, int n, const double* y, double* dfdx, double* 
 int gf_lu_decompose(int n_mats, int m, double* A, int* pivots, void* stream) {
     if (n_mats < 0 || m < 1 || m > 160 || (n_mats > 0 && (!A || !pivots))) return GF_ERR_INVALID_ARGUMENT;
     const int e = gf::launch_lu(n_mats, m, A, pivots, nullptr, stream);
+    return e ? cuda_fail((cudaError_t)e) : GF_OK;
+}
+
+int gf_lu_factor_solve(int n_mats, int m, double* A, int* pivots, double* b, int n_rhs, int threads_per_matrix,
+                       int exact, void* stream) {
+    const int G = threads_per_matrix;
+    if (G != 1 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 128 && G != 256)
+        return GF_ERR_INVALID_ARGUMENT;
+    if (n_mats < 0 || m < 1 || m > 160 || n_rhs < 0 || (n_mats > 0 && (!A || !pivots || (n_rhs > 0 && !b))))
+        return GF_ERR_INVALID_ARGUMENT;
+    const int e = gf::launch_lu_form(n_mats, m, A, pivots, b, n_rhs, G, exact != 0, stream);
     return e ? cuda_fail((cudaError_t)e) : GF_OK;
 }
 

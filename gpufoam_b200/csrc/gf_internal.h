@@ -174,6 +174,8 @@ int launch_jacobian(const DevMech& m, int n, const double* y, double* dfdx, doub
                     void* stream);
 int launch_lu(int n_mats, int m, double* A, int* piv, double* vv, void* stream);
 int launch_lusolve(int n_mats, int m, const double* LU, const int* piv, double* b, void* stream);
+// The production factorisation and solves (lu_factor, lu_solve_any) with G threads per matrix.
+int launch_lu_form(int n_mats, int m, double* A, int* piv, double* b, int n_rhs, int G, int exact, void* stream);
 int launch_epilogue_reset(unsigned long long* queue, void* stream);
 
 // The discrete adjoint (gf_adjoint.cu).
@@ -207,8 +209,11 @@ int launch_gather_states(int n, int nS, const double* const* Y, const double* T,
                          void* stream);
 int launch_scatter_rates(int n, int nS, const double* RR, int ld, double* const* out, void* stream);
 
-// Device tables of a mechanism object (gf_host.cpp).
+// Device tables of a mechanism object and the device that holds them (gf_host.cpp).
 const DevMech* mech_device_tables(const gf_mech* m);
+int mech_device(const gf_mech* m);
+// Keeps the CUDA error's text for gf_last_cuda_error and returns its gf_status.
+int record_cuda_error(int cuda_error);
 
 // Resident-slot count for a persistent configuration (groups that run at once).
 int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* blocks_out, int* threads_out);

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(128) plain_kernel(const MechSet P, const Launc
     Grp<1> g;
     const DevMech* M = pick(P, a, cell);
     if (!M) {
-        reject_cell(a, cell);
+        reject_cell(g, a, cell);
         return;
     }
     WsS w{a.ws + cell, a.ws_slot_stride};
@@ -111,7 +111,73 @@ __global__ void __launch_bounds__(32) lusolve_kernel(int m, const double* LU, co
     for (int i = g.lane; i < m; i += 32) b[(size_t)blockIdx.x * m + i] = w[ob + i];
 }
 
+// The factorisation and the solves exactly as the solve kernels run them
+// (lu_factor, lu_solve_any) with a group of G threads per matrix: after the
+// row scaling of LUDecompose, the register-panel form (G >= 32, m <= 64) or the
+// blocked one, reciprocal pivots for G >= 16; EXACT rounds every update a - l u
+// twice, as the reference's CPU build does. One matrix per CTA; A [m][m] is
+// replaced by its factors, b [n_rhs][m] by the solutions.
+template <int G, bool EXACT>
+__global__ void __launch_bounds__(G < 32 ? 32 : G) lu_form_kernel(int m, double* A, int* piv, double* b, int n_rhs) {
+    extern __shared__ double smem[];
+    Grp<G> g;
+    if (G < 32 && threadIdx.x >= G) return;
+    const int ld = m | 1;
+    WsC w{smem};
+    const int oA = 0, ovv = m * ld, opiv = ovv + m, operm = opiv + m, ob = operm + m;
+    double* Ag = A + (size_t)blockIdx.x * m * m;
+    for (int e = g.lane; e < m * m; e += G) w[oA + (e / m) * ld + (e % m)] = Ag[e];
+    g.sync();
+    row_scale(g, w, oA, ld, ovv, m);
+    lu_factor<G, EXACT>(g, w, oA, ld, opiv, ovv, operm, m);
+    g.sync();
+    for (int e = g.lane; e < m * m; e += G) Ag[e] = w[oA + (e / m) * ld + (e % m)];
+    for (int i = g.lane; i < m; i += G) piv[(size_t)blockIdx.x * m + i] = w.ip(opiv + i);
+    for (int r = 0; r < n_rhs; ++r) {
+        double* bg = b + ((size_t)blockIdx.x * n_rhs + r) * m;
+        g.sync();
+        for (int i = g.lane; i < m; i += G) w[ob + i] = bg[i];
+        g.sync();
+        lu_solve_any(g, w, oA, ld, opiv, operm, ovv, m, ob);
+        g.sync();
+        for (int i = g.lane; i < m; i += G) bg[i] = w[ob + i];
+    }
+}
+
+template <int G, bool EXACT>
+static int launch_lu_form_g(int n_mats, int m, double* A, int* piv, double* b, int n_rhs, cudaStream_t s) {
+    const size_t smem = ((size_t)m * (m | 1) + 4 * (size_t)m) * sizeof(double);
+    const void* fn = reinterpret_cast<const void*>(&lu_form_kernel<G, EXACT>);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    lu_form_kernel<G, EXACT><<<n_mats, G < 32 ? 32 : G, smem, s>>>(m, A, piv, b, n_rhs);
+    return (int)cudaGetLastError();
+}
+
+template <int G>
+static int launch_lu_form_e(int n_mats, int m, double* A, int* piv, double* b, int n_rhs, int exact,
+                            cudaStream_t s) {
+    return exact ? launch_lu_form_g<G, true>(n_mats, m, A, piv, b, n_rhs, s)
+                 : launch_lu_form_g<G, false>(n_mats, m, A, piv, b, n_rhs, s);
+}
+
 // ---------------------------------------------------------------- launchers
+
+int launch_lu_form(int n_mats, int m, double* A, int* piv, double* b, int n_rhs, int G, int exact, void* stream) {
+    if (n_mats <= 0) return 0;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    switch (G) {
+    case 1: return launch_lu_form_e<1>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 4: return launch_lu_form_e<4>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 8: return launch_lu_form_e<8>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 16: return launch_lu_form_e<16>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 32: return launch_lu_form_e<32>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 64: return launch_lu_form_e<64>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 128: return launch_lu_form_e<128>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 256: return launch_lu_form_e<256>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
 
 WsLayout ws_layout(const DevMech& m) { return make_layout(m.nS, m.nR, m.n_slots, m.n_tb); }
 

@@ -1,7 +1,9 @@
 // gf_solve_noalloc: the per-flow-step chemistry solve without any device
-// allocation, for callers that cannot call cudaMalloc (code that runs while a
-// CUDA graph is being captured, host codes whose device memory is owned by
-// another allocator, or real-time loops that forbid allocation after start-up).
+// allocation, for callers that cannot call cudaMalloc: a host code whose device
+// memory belongs to another allocator (a caching pool that has reserved the
+// free memory, or a host application that requires every allocation to go
+// through its own memory manager), or a real-time loop that forbids
+// allocation once it has started.
 //
 // Every other solve entry point keeps its scratch (per-cell workspaces and the
 // work-queue counters) in device memory that gf_solver_create / gf_solve
@@ -22,6 +24,10 @@
 // every call (on the caller's stream), the workspaces need no clearing, and
 // calls whose kernels overlap on a GPU (different streams, or different host
 // threads on the same device) race on the arrays and must not be issued.
+//
+// With stats != NULL the call copies the step totals to the host and waits for
+// the caller's stream; it then refuses a stream that is being captured
+// (GF_ERR_INVALID_ARGUMENT), whose capture that wait would invalidate.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -69,17 +75,16 @@ __global__ void noalloc_reset(unsigned long long* q) {
     q[4] = 0;
 }
 
-int symbol_addresses(SymbolAddrs* out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return GF_ERR_NO_DEVICE;
+int symbol_addresses(int dev, SymbolAddrs* out) {
     if (dev < 0 || dev >= kMaxDevices) return GF_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_addrs_mutex);
     SymbolAddrs& s = g_addrs[dev];
     if (!s.ws) {
         void* ws = nullptr;
         void* q = nullptr;
-        if (cudaGetSymbolAddress(&ws, g_noalloc_ws) != cudaSuccess) return GF_ERR_CUDA;
-        if (cudaGetSymbolAddress(&q, g_noalloc_queue) != cudaSuccess) return GF_ERR_CUDA;
+        cudaError_t e = cudaGetSymbolAddress(&ws, g_noalloc_ws);
+        if (e == cudaSuccess) e = cudaGetSymbolAddress(&q, g_noalloc_queue);
+        if (e != cudaSuccess) return gf::record_cuda_error((int)e);
         s.ws = static_cast<double*>(ws);
         s.queue = static_cast<unsigned long long*>(q);
     }
@@ -98,16 +103,29 @@ extern "C" int gf_solve_noalloc(const gf_mech* mech, const gf_ode_inputs* in, do
         return GF_ERR_UNKNOWN_SOLVER;
     const gf::DevMech* M = gf::mech_device_tables(mech);
     if (ld_y < M->nS + 2 || (RR && (!rho || ld_rr < M->nS))) return GF_ERR_INVALID_ARGUMENT;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return gf::record_cuda_error((int)e);
+    // the mechanism's tables must be on the current device
+    if (dev != gf::mech_device(mech)) return GF_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (stats) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        e = cudaStreamIsCapturing(s, &cs);
+        if (e != cudaSuccess) return gf::record_cuda_error((int)e);
+        if (cs != cudaStreamCaptureStatusNone) return GF_ERR_INVALID_ARGUMENT;
+    }
     const long long wsd = gf::ws_layout(*M).size;
     // the cap: workspaces of the resident cell groups must fit in the array
     long long groups_fit = kScratchDoubles / wsd;
     if (groups_fit < 1) return GF_ERR_UNSUPPORTED;
     SymbolAddrs addr;
-    int r = symbol_addresses(&addr);
+    int r = symbol_addresses(dev, &addr);
     if (r) return r;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, noalloc_kernel, 32, 0) != cudaSuccess || per_sm < 1)
-        return GF_ERR_CUDA;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, noalloc_kernel, 32, 0);
+    if (e != cudaSuccess) return gf::record_cuda_error((int)e);
+    if (per_sm < 1) return GF_ERR_UNSUPPORTED;
     const long long groups = std::min<long long>(groups_fit, (long long)per_sm * gf::device_sm_count());
     gf::LaunchArgs a;
     a.n_cells = n_cells;
@@ -130,15 +148,15 @@ extern "C" int gf_solve_noalloc(const gf_mech* mech, const gf_ode_inputs* in, do
     a.ws = addr.ws;
     a.ws_slot_stride = wsd;
     a.queue = addr.queue;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     noalloc_reset<<<1, 1, 0, s>>>(addr.queue);
     if (n_cells > 0) noalloc_kernel<<<(unsigned)groups, 32, 0, s>>>(*M, a, (int)wsd);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return GF_ERR_CUDA;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return gf::record_cuda_error((int)e);
     if (stats) {
         unsigned long long q[5];
-        if (cudaMemcpyAsync(q, addr.queue, sizeof(q), cudaMemcpyDeviceToHost, s) != cudaSuccess) return GF_ERR_CUDA;
-        if (cudaStreamSynchronize(s) != cudaSuccess) return GF_ERR_CUDA;
+        e = cudaMemcpyAsync(q, addr.queue, sizeof(q), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return gf::record_cuda_error((int)e);
         const unsigned long long k = q[1];
         const unsigned long long bits = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
         double mn;

@@ -30,9 +30,26 @@ __device__ __forceinline__ const DevMech* pick(const MechSet& P, const LaunchArg
     return (id >= 0 && id < P.n) ? &P.m[id] : nullptr;
 }
 
-__device__ __forceinline__ void reject_cell(const LaunchArgs& a, long long cell) {
-    if (a.status) a.status[cell] = GF_CELL_BAD_MECHANISM;
-    atomicAdd(a.queue + 4, 1ull);
+// Such a cell leaves the solve unchanged: its output row is a copy of its
+// input row (the whole row stride), its RR row is zero, its counters are zero
+// and its deltaTChem is left as it was; it is left out of the min over cells.
+template <int G>
+__device__ __forceinline__ void reject_cell(const Grp<G>& g, const LaunchArgs& a, long long cell) {
+    if (a.Ynew) {
+        const double* yi = a.Y0 + (size_t)cell * a.ld_y;
+        double* yo = a.Ynew + (size_t)cell * a.ld_y;
+        for (int i = g.lane; i < a.ld_y; i += G) yo[i] = yi[i];
+    }
+    if (a.RR)
+        for (int i = g.lane; i < a.ld_rr; i += G) a.RR[(size_t)cell * a.ld_rr + i] = 0.0;
+    if (g.lane == 0) {
+        if (a.status) a.status[cell] = GF_CELL_BAD_MECHANISM;
+        if (a.counters) {
+            a.counters[2 * cell] = 0;
+            a.counters[2 * cell + 1] = 0;
+        }
+        atomicAdd(a.queue + 4, 1ull);
+    }
 }
 
 // threads per CTA the kernel is compiled for
@@ -58,7 +75,7 @@ __global__ void __launch_bounds__(PersistShape<G>::kThreads, SLIM ? PersistShape
         if (cell >= a.n_cells) break;
         const DevMech* Mp = pick(P, a, cell);
         if (!Mp) {
-            if (g.lane == 0) reject_cell(a, cell);
+            reject_cell(g, a, cell);
             continue;
         }
         const DevMech& M = *Mp;

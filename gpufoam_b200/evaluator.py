@@ -175,16 +175,61 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
-def _check_rows(Y0, Ynew, RR, n):
-    """The solve writes Ynew with Y0's row stride and RR with its own: both must
-    be row-contiguous 2-D tensors of n rows (RR at least as wide as the species)."""
-    for name, t in (("Y0", Y0), ("Ynew", Ynew), ("RR", RR)):
+def check_solve_tensors(n, n_eqns, n_species, Y0, Ynew=None, RR=None, deltaTChem=None, rho=None,
+                        deltaT_cell=None, mech_id=None, status=None, counters=None):
+    """Every tensor a solve reads or writes, checked before the C ABI sees a
+    pointer (the kernels index them by cell with no size information):
+    float64 (int32 for mech_id, status, counters), the sizes the solve touches
+    (Y0/Ynew rows of at least n_eqns, RR rows of at least n_species, one value
+    per cell, counters [n][2]), contiguous rows, and all on Y0's CUDA device.
+    Raises ValueError."""
+    import torch
+    f64, i32 = torch.float64, torch.int32
+
+    def tensor(name, t):
+        if not isinstance(t, torch.Tensor):
+            raise ValueError(f"{name} must be a torch tensor")
+        return t
+
+    Y0 = tensor("Y0", Y0)
+    if Y0.dtype != f64:
+        raise ValueError("Y0 must be float64")
+    if Y0.dim() != 2 or Y0.shape[0] != n or Y0.shape[1] < n_eqns or Y0.stride(1) != 1:
+        raise ValueError(f"Y0 must be a row-contiguous [{n}][>= {n_eqns}] tensor")
+    rows = [("Ynew", Ynew, n_eqns), ("RR", RR, n_species)]
+    for name, t, width in rows:
         if t is None:
             continue
-        if t.dim() != 2 or t.shape[0] != n or t.stride(1) != 1:
-            raise ValueError(f"{name} must be a row-contiguous [n_cells][k] tensor")
+        tensor(name, t)
+        if t.dtype != f64:
+            raise ValueError(f"{name} must be float64")
+        if t.dim() != 2 or t.shape[0] != n or t.shape[1] < width or t.stride(1) != 1:
+            raise ValueError(f"{name} must be a row-contiguous [{n}][>= {width}] tensor")
     if Ynew is not None and (Ynew.shape[1] != Y0.shape[1] or Ynew.stride(0) != Y0.stride(0)):
         raise ValueError("Ynew must have Y0's shape and row stride")
+    per_cell = [("deltaTChem", deltaTChem, f64, 1), ("rho", rho, f64, 1), ("deltaT_cell", deltaT_cell, f64, 1),
+                ("mech_id", mech_id, i32, 1), ("status", status, i32, 1), ("counters", counters, i32, 2)]
+    for name, t, dtype, k in per_cell:
+        if t is None:
+            continue
+        tensor(name, t)
+        if t.dtype != dtype:
+            raise ValueError(f"{name} must be {dtype}")
+        if t.numel() < k * n or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous tensor of at least {k * n} values")
+    for name, t in [("Y0", Y0)] + [(nm, t) for nm, t, _ in rows] + [(nm, t) for nm, t, _, _ in per_cell]:
+        if t is not None and (not t.is_cuda or t.device != Y0.device):
+            raise ValueError(f"{name} must be on Y0's CUDA device")
+
+
+def check_host_arrays(n, n_eqns, Y, deltaTChem, rho=None, deltaT=None):
+    """Host arrays of computeRR / computeYNew: Y of n * n_eqns values, one
+    deltaTChem (and rho, deltaT) per cell. Raises ValueError."""
+    if Y.size != n * n_eqns:
+        raise ValueError(f"Y must hold nCells * nEqns = {n * n_eqns} values, not {Y.size}")
+    for name, a in (("deltaTChem", deltaTChem), ("rho", rho), ("deltaT", deltaT)):
+        if a is not None and a.shape != (n,):
+            raise ValueError(f"{name} must hold one value per cell ({n})")
 
 
 class Solver:
@@ -201,6 +246,7 @@ class Solver:
         self.ode = ode
         self.Treact = Treact
         self.max_neq = max(m.n_eqns for m in self.mechs)
+        self.max_species = max(m.n_species for m in self.mechs)
 
     def set_launch(self, kind=1, threads_per_cell=32, scratch_in_shared=1, cells_per_block=0, blocks_per_sm=0,
                    register_budget=0):
@@ -227,7 +273,8 @@ class Solver:
             RR = torch.empty((n, ld), dtype=torch.float64, device=Y0.device)
         status = torch.empty(n, dtype=torch.int32, device=Y0.device) if want_status else None
         counters = torch.empty((n, 2), dtype=torch.int32, device=Y0.device) if want_counters else None
-        _check_rows(Y0, Ynew, RR, n)
+        check_solve_tensors(n, self.max_neq, self.max_species, Y0, Ynew, RR, deltaTChem, rho, deltaT_cell, mech_id,
+                            status, counters)
         st = N.GfStats()
         N.check(self.lib.gf_solve(self.handle, n, float(deltaT), _ptr(deltaT_cell), float(deltaTChemMax),
                                   _ptr(mech_id), _ptr(rho), _ptr(Y0), ld, _ptr(Ynew), _ptr(deltaTChem), _ptr(RR),
@@ -248,7 +295,8 @@ class Solver:
             Ynew = torch.empty_like(Y0)
         if rho is not None and RR is None:
             RR = torch.empty((n, ld), dtype=torch.float64, device=Y0.device)
-        _check_rows(Y0, Ynew, RR, n)
+        check_solve_tensors(n, self.max_neq, self.max_species, Y0, Ynew, RR, deltaTChem, rho, deltaT_cell, mech_id,
+                            status, counters)
         h = C.c_void_p()
         N.check(self.lib.gf_solve_graph_create(self.handle, n, float(deltaT), _ptr(deltaT_cell), float(deltaTChemMax),
                                                _ptr(mech_id), _ptr(rho), _ptr(Y0), ld, _ptr(Ynew), _ptr(deltaTChem),
@@ -330,6 +378,7 @@ class GpuKernelEvaluator:
         dtc = np.ascontiguousarray(deltaTChem, dtype=np.float64)
         Yh = np.ascontiguousarray(Y, dtype=np.float64).reshape(-1)
         n = dtc.shape[0]
+        check_host_arrays(n, self.nEqns, Yh, dtc)
         Ynew = np.empty(n * self.nEqns)
         dtn = np.empty(n)
         N.check(self.lib.gf_compute_ynew(self.solver.handle, n, float(deltaT), float(deltaTChemMax),
@@ -344,6 +393,7 @@ class GpuKernelEvaluator:
         dtc = np.ascontiguousarray(deltaTChem, dtype=np.float64)
         Yh = np.ascontiguousarray(Y, dtype=np.float64).reshape(-1)
         n = rho.shape[0]
+        check_host_arrays(n, self.nEqns, Yh, dtc, rho)
         RR = np.empty(n * self.nSpecie)
         dtn = np.empty(n)
         mn = C.c_double()
@@ -361,8 +411,7 @@ class GpuKernelEvaluator:
         dtc = np.ascontiguousarray(deltaTChem, dtype=np.float64)
         Yh = np.ascontiguousarray(Y, dtype=np.float64).reshape(-1)
         n = rho.shape[0]
-        if dT.shape != (n,):
-            raise ValueError("deltaT must hold one value per cell")
+        check_host_arrays(n, self.nEqns, Yh, dtc, rho, dT)
         RR = np.empty(n * self.nSpecie)
         dtn = np.empty(n)
         mn = C.c_double()
@@ -379,10 +428,11 @@ def solve_noalloc(mech: Mechanism, ode: OdeInputs, Y0, deltaT: float, deltaTChem
     memory. Every array is the caller's (cuda tensors); deltaTChem is updated
     in place and Ynew/RR/status/counters are written. The library's static
     device scratch is shared by all calls, so calls must not overlap on a GPU.
-    Returns the statistics dict when stats=True (this synchronises the stream)."""
+    Returns the statistics dict when stats=True (this waits for the stream,
+    and is refused on a stream that is being captured)."""
     lib = N.load()
     n = int(Y0.shape[0])
-    _check_rows(Y0, Ynew, RR, n)
+    check_solve_tensors(n, mech.n_eqns, mech.n_species, Y0, Ynew, RR, deltaTChem, rho, None, None, status, counters)
     st = N.GfStats()
     N.check(lib.gf_solve_noalloc(mech.handle, C.byref(ode.to_c()), float(Treact), n, float(deltaT), None,
                                  float(deltaTChemMax), _ptr(rho), _ptr(Y0), int(Y0.stride(0)), _ptr(Ynew),
@@ -435,6 +485,24 @@ def lu_backsubstitute(LU, piv, b):
     N.check(lib.gf_lu_backsubstitute(k, m, _ptr(_dev(LU, torch.float64)), _ptr(_dev(piv, torch.int32)), _ptr(bd),
                                      _stream_ptr()), "gf_lu_backsubstitute")
     return bd
+
+
+def lu_factor_solve(A, b, threads_per_matrix: int, exact: bool = False):
+    """LUDecompose + LUBacksubstitute as the solve kernels run them with
+    threads_per_matrix threads per matrix (gf_lu_factor_solve): A [k][m][m],
+    b [k][n_rhs][m] (host or device) -> (factors, pivots, solutions), cuda tensors.
+    exact=True rounds each elimination update twice (no FMA contraction)."""
+    import torch
+    lib = N.load()
+    Ad = _dev(A, torch.float64).clone()
+    bd = _dev(b, torch.float64).clone()
+    k, m, _ = Ad.shape
+    if bd.dim() != 3 or bd.shape[0] != k or bd.shape[2] != m:
+        raise ValueError("b must be [n_mats][n_rhs][m]")
+    piv = torch.empty((k, m), dtype=torch.int32, device="cuda")
+    N.check(lib.gf_lu_factor_solve(k, m, _ptr(Ad), _ptr(piv), _ptr(bd), int(bd.shape[1]), int(threads_per_matrix),
+                                   int(bool(exact)), _stream_ptr()), "gf_lu_factor_solve")
+    return Ad, piv, bd
 
 
 # ---- the plugin's per-cell side paths (gpuChemistryModel.C:145-450), on the GPU

@@ -386,11 +386,15 @@ def coverage(seed: int = 0) -> RawMechanism:
 
 def make_cells(mech: RawMechanism, n_cells: int, seed: int = 0, T_range=(1000.0, 2500.0),
                p: float = 101325.0, bimodal: Optional[Tuple[float, Tuple[float, float], Tuple[float, float]]] = None,
-               p_range: Optional[Tuple[float, float]] = None, dirichlet_alpha: float = 0.5) -> np.ndarray:
+               p_range: Optional[Tuple[float, float]] = None, dirichlet_alpha: float = 0.5,
+               cold_reactive_fraction: Optional[float] = None) -> np.ndarray:
     """[n_cells, nS + 2] cell states (Y..., T, p), cell-major.
 
     bimodal = (fraction_cold, (Tlo, Thi)_cold, (Tlo, Thi)_hot): cells drawn cold
-    or hot, then shuffled by the seed.
+    or hot, then shuffled by the seed. cold_reactive_fraction (bimodal only):
+    the cold cells are near-inert, their Dirichlet composition scaled to this
+    total mass fraction and the rest given to the inert species (the last
+    one); None leaves every cell's Dirichlet composition as drawn.
     """
     rng = np.random.default_rng(seed)
     nS = mech.n_species
@@ -403,7 +407,13 @@ def make_cells(mech: RawMechanism, n_cells: int, seed: int = 0, T_range=(1000.0,
         n_cold = int(round(frac * n_cells))
         T = np.concatenate([rng.uniform(cold[0], cold[1], size=n_cold),
                             rng.uniform(hot[0], hot[1], size=n_cells - n_cold)])
-        T = T[rng.permutation(n_cells)]
+        is_cold = np.arange(n_cells) < n_cold
+        order = rng.permutation(n_cells)
+        T, is_cold = T[order], is_cold[order]
+        if cold_reactive_fraction is not None:
+            eps = float(cold_reactive_fraction)
+            Y[is_cold] *= eps
+            Y[is_cold, nS - 1] += 1.0 - eps
     if p_range is None:
         P = np.full(n_cells, p)
     else:

@@ -28,6 +28,7 @@
  *   gf_jacobian              gpuODESystem::jacobian         gpu_chemistry/src/gpuOde/gpuODESystem.H:198-281
  *   gf_lu_decompose          LUDecompose                    gpu_chemistry/src/gpuOde/ludecompose.H:9-92
  *   gf_lu_backsubstitute     LUBacksubstitute               gpu_chemistry/src/gpuOde/ludecompose.H:94-130
+ *   gf_lu_factor_solve       LUDecompose + LUBacksubstitute ludecompose.H:9-130 (the solve kernels' forms)
  */
 #ifndef GPUFOAM_B200_H
 #define GPUFOAM_B200_H
@@ -197,7 +198,9 @@ int gf_solver_get_launch(const gf_solver* solver, gf_launch_config* cfg);
  *   deltaT_cell    per-cell time step [n_cells] or NULL (local time stepping)
  *   deltaTChemMax  clamp for the returned chemistry time steps
  *   mech_id        per-cell mechanism index [n_cells] or NULL (all mechanism 0); a cell whose
- *                  id is outside 0 .. n_mechs-1 is not integrated (GF_CELL_BAD_MECHANISM)
+ *                  id is outside 0 .. n_mechs-1 is not integrated (GF_CELL_BAD_MECHANISM):
+ *                  its Ynew row is a copy of its Y0 row, its RR row zero, its counters
+ *                  zero, its deltaTChem unchanged, and it counts as a failed cell
  *   rho            old-time density [n_cells] (may be NULL when RR is NULL)
  *   Y0             input states [n_cells][nEqns of the cell's mechanism], row stride ld_y
  *   Ynew           output states, same layout (may alias Y0, may be NULL)
@@ -238,7 +241,9 @@ void gf_solve_graph_destroy(gf_solve_graph* graph);
 
 /* Host-memory mirror of GpuKernelEvaluator::computeRR (single mechanism):
  * RR [n_cells][nSpecie], deltaTChemNew [n_cells] (clamped), *minDeltaT (before
- * clamping). Copies in and out through pinned staging owned by the solver. */
+ * clamping). The host arrays are copied to and from device staging buffers
+ * that the solver allocates on first use (cudaMalloc) and keeps; the copies
+ * run at pageable-memory speed unless the caller's arrays are pinned. */
 int gf_compute_rr(gf_solver* solver, int n_cells, double deltaT, double deltaTChemMax,
                   const double* rho, const double* deltaTChem, const double* Y,
                   double* RR, double* deltaTChemNew, double* minDeltaT);
@@ -328,17 +333,21 @@ int gf_adjoint(gf_solver* solver, int n_cells, const double* traj, int traj_cap,
 #define GF_NOALLOC_SCRATCH_BYTES (32ll * 1024 * 1024)
 
 /* gf_solve without any device allocation — no counterpart in the reference.
- * For callers that cannot call cudaMalloc: code that runs while a CUDA graph is
- * captured, host codes whose device memory belongs to another allocator,
- * loops that forbid allocation after start-up. The mechanism (gf_mech_create)
- * is set-up-time input; inputs and outputs are the caller's device arrays, as
- * in gf_solve. The per-cell workspaces and work-queue counters live in a static
+ * For callers that cannot call cudaMalloc: a host code whose device memory
+ * belongs to another allocator (a caching pool that has reserved the free
+ * memory, or a host application that requires every allocation to go through
+ * its own memory manager), or a real-time loop that forbids allocation once it
+ * has started. The mechanism (gf_mech_create, on the current device) is
+ * set-up-time input; inputs and outputs are the caller's device arrays, as in
+ * gf_solve. The per-cell workspaces and work-queue counters live in a static
  * device array of GF_NOALLOC_SCRATCH_BYTES that every GPU loading the library
  * holds until exit; the number of cells integrated at once is capped so their
  * workspaces fit (GF_ERR_UNSUPPORTED if not even one cell's does). The first
  * call on each device resolves the array's address (cudaGetSymbolAddress) and
  * should come before any stream capture. All calls share the array: calls
- * whose kernels overlap on one GPU race and must not be issued. */
+ * whose kernels overlap on one GPU race and must not be issued. With stats !=
+ * NULL the call copies the step totals to the host and waits for the stream;
+ * it returns GF_ERR_INVALID_ARGUMENT for a stream that is being captured. */
 int gf_solve_noalloc(const gf_mech* mech, const gf_ode_inputs* inputs, double Treact, int n_cells, double deltaT,
                      const double* deltaT_cell, double deltaTChemMax, const double* rho, const double* Y0, int ld_y,
                      double* Ynew, double* deltaTChem, double* RR, int ld_rr, int* status, int* counters,
@@ -358,6 +367,18 @@ int gf_lu_decompose(int n_mats, int m, double* A, int* pivots, void* stream);
 /* In-place solve of b [n_mats][m] with the factors from gf_lu_decompose. */
 int gf_lu_backsubstitute(int n_mats, int m, const double* LU, const int* pivots,
                          double* b, void* stream);
+
+/* LUDecompose + LUBacksubstitute (ludecompose.H:9-130) as the solve kernels
+ * run them, with threads_per_matrix (1, 4, 8, 16, 32, 64, 128 or 256) threads
+ * per matrix: after the implicit row scaling, the register-panel factorisation
+ * for 32 or more threads and m <= 64, the blocked one otherwise; solves by
+ * reciprocal pivots for 16 or more threads. exact != 0 rounds every
+ * elimination update a - l u twice (no FMA contraction), as the reference's
+ * CPU build computes its Crout sums, so the factors can be compared bit for
+ * bit. A [n_mats][m][m] (in place: the factors), pivots [n_mats][m],
+ * b [n_mats][n_rhs][m] (in place: the solutions); m <= 160; device pointers. */
+int gf_lu_factor_solve(int n_mats, int m, double* A, int* pivots, double* b, int n_rhs,
+                       int threads_per_matrix, int exact, void* stream);
 
 /* ---- measurement (no reference counterpart) -------------------------------- */
 

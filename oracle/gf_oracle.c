@@ -1008,7 +1008,7 @@ void orc_cells(void* h, const orc_ode_inputs* o, double Treact, int nc, double d
         ws_t w;
         ws_init(&w, nS);
 #ifdef _OPENMP
-#pragma omp for schedule(dynamic, 64)
+#pragma omp for schedule(dynamic, 1)
 #endif
         for (int c = 0; c < nc; ++c) {
             double* y = Y + (size_t)n * c;

@@ -20,6 +20,10 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the gpuFoam source tree: GPUFOAM_REFERENCE, else a directory named reference
+# beside this repository (the same rule as oracle/Makefile)
+REFERENCE_ROOT = os.environ.get("GPUFOAM_REFERENCE",
+                                os.path.normpath(os.path.join(HERE, "..", "..", "reference")))
 PORT_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libgf_ref.so")
 
@@ -45,7 +49,7 @@ def ode_inputs(solver=34, absTol=1e-8, relTol=1e-4, maxSteps=10000, safeScale=0.
 def build(force: bool = False) -> None:
     """Build the oracles (make -C oracle)."""
     if force or not os.path.exists(PORT_LIB) or (
-            os.path.isdir("/root/reference/gpu_chemistry") and not os.path.exists(REF_LIB)):
+            os.path.isdir(os.path.join(REFERENCE_ROOT, "gpu_chemistry")) and not os.path.exists(REF_LIB)):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 

@@ -15,7 +15,7 @@
 //  * a counting wrapper around the reference Rosenbrock solvers so that the
 //    accepted/attempted substeps of odeSolve can be compared per cell;
 //  * the host-side computeRR arithmetic (gpuKernelEvaluator.cu:65-97);
-//  * an OpenMP loop over cells (schedule(dynamic,64)) for the timed CPU
+//  * an OpenMP loop over cells (schedule(dynamic,1): one cell per chunk) for the timed CPU
 //    baseline.
 #include <cmath>
 #include <cstring>
@@ -336,7 +336,7 @@ void ref_cells_counted(void* h, const OdeIn* o, double Treact, int n, double del
         {
             Buf buf(nS);
             auto ode = ode_proto;
-#pragma omp for schedule(dynamic, 64)
+#pragma omp for schedule(dynamic, 1)
             for (int c = 0; c < n; ++c) {
                 ode.accepted = 0;
                 ode.attempts = 0;
@@ -371,7 +371,7 @@ void ref_cells(void* h, const OdeIn* o, double Treact, int n, double deltaT, dou
 #pragma omp parallel num_threads(nthreads > 0 ? nthreads : omp_get_max_threads())
     {
         Buf buf(nS);
-#pragma omp for schedule(dynamic, 64)
+#pragma omp for schedule(dynamic, 1)
         for (int c = 0; c < n; ++c) {
             // one-cell views so that each thread uses its own scratch buffer
             auto Ys = mdspan<gScalar, 2>(Y + ne * c, extents<2>{1, ne});

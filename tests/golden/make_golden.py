@@ -1,7 +1,8 @@
 """Generate the golden fixtures of tests/golden/ from the gpuFoam reference.
 
-Run in a container where the reference tree exists (its FP64 headers are
-compiled in place by oracle/Makefile into oracle/_ref/libgf_ref.so):
+Run where the reference tree exists (GPUFOAM_REFERENCE, else a directory
+named reference beside this repository; its FP64 headers are compiled in
+place by oracle/Makefile into oracle/_ref/libgf_ref.so):
 
     python tests/golden/make_golden.py
 
@@ -26,7 +27,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 from gpufoam_b200 import mechanism as M  # noqa: E402
-from oracle.oracle import Oracle, flatten, lu, ode_inputs  # noqa: E402
+from oracle.oracle import REFERENCE_ROOT, Oracle, flatten, lu, ode_inputs  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 
@@ -42,8 +43,7 @@ CASES = [
 # gpufoam_b200.foam_dict, with the reference's own test condition
 # (testHelpers/mechanisms.H:36-107: T = 1000 K, the mechanism's p and three
 # non-zero mass fractions) as state 0.
-REF = os.environ.get("GPUFOAM_REFERENCE", "/root/reference")
-HELPERS = os.path.join(REF, "gpu_chemistry", "unittest", "testHelpers")
+HELPERS = os.path.join(REFERENCE_ROOT, "gpu_chemistry", "unittest", "testHelpers")
 FOAM = [
     # name, file stem, (species index, Y) of the test condition, p, n states, n cells, deltaT
     ("foam_h2", "h2", [(0, 0.2), (2, 0.2), (9, 0.6)], 202650.0, 8, 32, 1e-5),
@@ -127,10 +127,53 @@ def make_lu():
     print("lu written")
 
 
+def make_lu_forms():
+    """LUDecompose + LUBacksubstitute of the reference at the sizes the solve
+    kernels' forms switch at (m <= 64 register panel, larger blocked; the
+    10-, 53- and 100-species mechanisms give m = 11, 54, 101), on four kinds of
+    matrices: uniform entries, small integers (exact ties of vv |a|, the "last
+    max wins" rule, and zero pivots), a zero column (the gpuSmall pivot), and
+    the Rosenbrock matrices I / (gamma dx) - J of real Jacobians."""
+    rng = np.random.default_rng(17)
+    out = {"sizes": np.array([11, 12, 33, 54, 55, 64, 65, 101])}
+    jac = {}
+    for factory in (M.h2_size, M.gri_size, M.large):
+        mech = factory(0)
+        states = M.make_cells(mech, 2, seed=23)
+        _, J = Oracle(mech, "reference").jacobian(states)
+        m = mech.n_species + 1
+        jac[m] = J[:, :m, :m]
+    kinds = []
+    for m in out["sizes"]:
+        mats = {"uniform": rng.uniform(size=(1, m, m)),
+                "ties": rng.integers(-3, 4, size=(1, m, m)).astype(np.float64)}
+        z = rng.uniform(-1.0, 1.0, size=(1, m, m))
+        z[:, :, m // 3] = 0.0
+        mats["zerocol"] = z
+        if m in jac:
+            dx = np.array([1e-9, 1e-6])
+            mats["rosenbrock"] = -jac[m] + np.eye(m)[None] / (0.5 * dx[:, None, None])
+        for kind, A in mats.items():
+            b = np.stack([np.ones((A.shape[0], m)), rng.standard_normal((A.shape[0], m))], axis=1)
+            xs = []
+            for r in range(2):
+                LU, piv, x = lu("reference", A, b[:, r])
+                xs.append(x)
+            key = f"{kind}_{m}"
+            kinds.append(key)
+            out[f"A_{key}"], out[f"b_{key}"] = A, b
+            out[f"LU_{key}"], out[f"piv_{key}"], out[f"x_{key}"] = LU, piv, np.stack(xs, axis=1)
+    out["cases"] = np.array(kinds)
+    np.savez_compressed(os.path.join(OUT, "lu_forms.npz"), **out)
+    print("lu_forms written", len(kinds), "cases")
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     if not only or "lu" in only:
         make_lu()
+    if not only or "lu_forms" in only:
+        make_lu_forms()
     for case in CASES:
         if not only or case[0] in only:
             make_case(*case)

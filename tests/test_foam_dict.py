@@ -10,12 +10,11 @@ import pytest
 
 from gpufoam_b200 import foam_dict as F
 from gpufoam_b200 import mechanism as M
-from oracle.oracle import flatten
+from oracle.oracle import REFERENCE_ROOT, flatten
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-HELPERS = os.path.join(os.environ.get("GPUFOAM_REFERENCE", "/root/reference"), "gpu_chemistry", "unittest",
-                       "testHelpers")
+HELPERS = os.path.join(REFERENCE_ROOT, "gpu_chemistry", "unittest", "testHelpers")
 
 THERMO = """
 FoamFile { format ascii; class dictionary; }   // header, ignored

@@ -130,7 +130,7 @@ def test_grisize_cells_vs_oracle(torch):
         Y, dtc, cnt, st, _ = run_cells(torch, mech, cells, 1e-6, 1e-7, 23, LAUNCHES[launch])
         assert (st == 0).all()
         assert_states_close(Y, ref[0], raw.n_species, 1e-4, launch)
-        assert step_count_agreement(cnt, ref[2]) >= 0.97
+        assert step_count_agreement(cnt, ref[2]) >= 0.99
 
 
 def test_compute_rr_mirror(torch):
@@ -268,7 +268,7 @@ def test_mixed_mechanisms_per_cell_dt(torch):
         sel = mid == k
         ref = Oracle(r, "port").cells(ode_inputs(34), Y[sel, :r.n_eqns], 0.0, 1e-7, deltaT_cell=dts[sel])
         assert_states_close(Yg[sel, :r.n_eqns], ref[0], r.n_species, 1e-4, f"mech {k}")
-        assert step_count_agreement(cnt[sel], ref[2]) >= 0.97
+        assert step_count_agreement(cnt[sel], ref[2]) >= 0.99
 
 
 def test_graph_replay_matches_solve(torch):

@@ -109,18 +109,54 @@ def test_null_handles_rejected_without_a_device(lib):
     assert lib.gf_qdot(None, 4, None, 10, None, None) == 1
 
 
-def test_solve_row_checks():
-    """Solver.solve / capture refuse output tensors whose rows the kernel would
-    overrun (the row strides are passed to the C ABI as given)."""
+def test_solve_tensor_checks():
+    """The solve wrappers refuse, before any pointer reaches the C ABI, a tensor
+    the kernels would read or write past its end, one of the wrong type, and one
+    that is not on Y0's CUDA device (on this machine every tensor is on the
+    CPU, so a tensor that passes the type and size checks fails the device one)."""
     import torch
-    Y0 = torch.zeros((4, 12), dtype=torch.float64)
-    E._check_rows(Y0, torch.zeros_like(Y0), torch.zeros((4, 10), dtype=torch.float64), 4)
-    with pytest.raises(ValueError):
-        E._check_rows(Y0, torch.zeros((4, 11), dtype=torch.float64), None, 4)
-    with pytest.raises(ValueError):
-        E._check_rows(Y0, None, torch.zeros((3, 10), dtype=torch.float64), 4)
-    with pytest.raises(ValueError):
-        E._check_rows(Y0, None, torch.zeros((10, 4), dtype=torch.float64).t(), 4)
+    f64, i32 = torch.float64, torch.int32
+    n, ne, ns = 4, 12, 10
+    Y0 = torch.zeros((n, ne), dtype=f64)
+
+    def refused(match, **kw):
+        with pytest.raises(ValueError, match=match):
+            E.check_solve_tensors(n, ne, ns, kw.pop("Y0", Y0), **kw)
+
+    # type and size failures, each caught before the device check
+    refused("Y0 must be float64", Y0=Y0.float())
+    refused("Y0 must be a row-contiguous", Y0=torch.zeros((n, ne - 1), dtype=f64))
+    refused("Y0 must be a row-contiguous", Y0=torch.zeros((ne, n), dtype=f64).t())
+    refused("Ynew must be a row-contiguous", Ynew=torch.zeros((n, ne - 1), dtype=f64))
+    refused("Ynew must have Y0's shape", Ynew=torch.zeros((n, ne + 2), dtype=f64))
+    refused("RR must be a row-contiguous", RR=torch.zeros((n - 1, ns), dtype=f64))
+    refused("RR must be a row-contiguous", RR=torch.zeros((n, ns - 1), dtype=f64))
+    refused("RR must be float64", RR=torch.zeros((n, ns), dtype=torch.float32))
+    refused("deltaTChem must be torch.float64", deltaTChem=torch.zeros(n, dtype=torch.float32))
+    refused("deltaTChem must be a contiguous tensor of at least 4", deltaTChem=torch.zeros(n - 1, dtype=f64))
+    refused("rho must be a contiguous tensor", rho=torch.zeros(2 * n, dtype=f64)[::2])
+    refused("deltaT_cell must be a contiguous tensor", deltaT_cell=torch.zeros(1, dtype=f64))
+    refused("mech_id must be torch.int32", mech_id=torch.zeros(n, dtype=torch.int64))
+    refused("status must be a contiguous tensor", status=torch.zeros(n - 1, dtype=i32))
+    refused("counters must be a contiguous tensor of at least 8", counters=torch.zeros((n, 1), dtype=i32))
+    refused("must be a torch tensor", deltaTChem=np.zeros(n))
+    # right types and sizes: only the device is wrong here
+    refused("must be on Y0's CUDA device", Ynew=torch.zeros_like(Y0), RR=torch.zeros((n, ns), dtype=f64),
+            deltaTChem=torch.zeros(n, dtype=f64), rho=torch.zeros(n, dtype=f64),
+            mech_id=torch.zeros(n, dtype=i32), status=torch.zeros(n, dtype=i32),
+            counters=torch.zeros((n, 2), dtype=i32))
+
+
+def test_host_array_checks():
+    """computeRR / computeYNew refuse host arrays whose sizes do not match nCells."""
+    n, ne = 5, 12
+    E.check_host_arrays(n, ne, np.zeros(n * ne), np.zeros(n), np.zeros(n), np.zeros(n))
+    with pytest.raises(ValueError, match="nCells"):
+        E.check_host_arrays(n, ne, np.zeros(n * ne - 1), np.zeros(n))
+    with pytest.raises(ValueError, match="rho"):
+        E.check_host_arrays(n, ne, np.zeros(n * ne), np.zeros(n), np.zeros(n + 1))
+    with pytest.raises(ValueError, match="deltaT "):
+        E.check_host_arrays(n, ne, np.zeros(n * ne), np.zeros(n), np.zeros(n), np.zeros(n - 1))
 
 
 @pytest.mark.parametrize("name", ["h2size", "coverage", "grisize", "foam_h2", "foam_gri", "foam_yao"])
