@@ -32,7 +32,7 @@ EXPORTS = [
     "gf_solve_record", "gf_adjoint", "gf_solve_graph_create", "gf_solve_graph_set_delta_t",
     "gf_solve_graph_launch", "gf_solve_graph_stats", "gf_solve_graph_destroy", "gf_cell_rates",
     "gf_reaction_rates", "gf_qdot", "gf_gather_states", "gf_scatter_rates", "gf_compute_rr_lts",
-    "gf_lu_factor_solve",
+    "gf_lu_factor_solve", "gf_solver_info",
 ]
 
 
@@ -120,6 +120,7 @@ def load() -> C.CDLL:
     lib.gf_solver_destroy.restype = None
     lib.gf_solver_set_launch.argtypes = [vp, P(GfLaunchConfig)]
     lib.gf_solver_get_launch.argtypes = [vp, P(GfLaunchConfig)]
+    lib.gf_solver_info.argtypes = [vp, P(ip), P(ip), P(ip)]
     lib.gf_solve.argtypes = [vp, ip, dp, vp, dp, vp, vp, vp, ip, vp, vp, vp, ip, vp, vp, P(GfStats), vp]
     lib.gf_compute_rr.argtypes = [vp, ip, dp, dp, vp, vp, vp, vp, vp, P(dp)]
     lib.gf_compute_ynew.argtypes = [vp, ip, dp, dp, vp, vp, vp, vp]

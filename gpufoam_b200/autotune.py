@@ -8,8 +8,9 @@ offers on a sample of the caller's cells and keeps the fastest:
     inside a warp) or 64, 128, 256 (one cell per CTA), the per-cell workspace in
     shared memory (when it fits) or in HBM, and two register budgets.
 
-Results are cached per (device, mechanism shape, solver) in memory and in a
-JSON file (GPUFOAM_AUTOTUNE_CACHE, default ~/.cache/gpufoam_b200/autotune.json).
+Results are cached per (device, library build, mechanism shape, solver) in
+memory and in a JSON file (GPUFOAM_AUTOTUNE_CACHE, default
+~/.cache/gpufoam_b200/autotune.json); a rebuilt library tunes afresh.
 """
 from __future__ import annotations
 
@@ -30,10 +31,28 @@ def _cache_path() -> str:
                           os.path.join(os.path.expanduser("~"), ".cache", "gpufoam_b200", "autotune.json"))
 
 
+_BUILD_HASH: Optional[str] = None
+
+
+def build_hash() -> str:
+    """Digest of the loaded library file: a cached pick is only reused with the
+    kernels it was timed on."""
+    global _BUILD_HASH
+    if _BUILD_HASH is None:
+        from . import _native as N
+        h = hashlib.sha1()
+        with open(N.LIB_PATH, "rb") as f:
+            for block in iter(lambda: f.read(1 << 20), b""):
+                h.update(block)
+        _BUILD_HASH = h.hexdigest()[:16]
+    return _BUILD_HASH
+
+
 def _key(mechs, ode: E.OdeInputs) -> str:
     import torch
     h = hashlib.sha1()
     h.update(torch.cuda.get_device_name().encode())
+    h.update(build_hash().encode())
     for m in mechs:
         h.update(f"{m.n_species}/{m.n_reactions}/{m.raw.name}".encode())
     h.update(f"{ode.name}/{ode.relTol}/{ode.absTol}".encode())
@@ -107,7 +126,7 @@ def tune(solver: E.Solver, Y_sample, deltaT: float, dtc0: float = 1e-7, deltaT_c
             pass
     Y0 = torch.as_tensor(Y_sample, dtype=torch.float64, device="cuda").contiguous()
     d0 = torch.full((Y0.shape[0],), dtc0, dtype=torch.float64, device="cuda")
-    ws = max(_ws_doubles(m) for m in solver.mechs)
+    ws = solver.workspace_doubles()
     table = []
     cands = configs or candidates(ws)
     # the usual winners first, so that slow forms are cut off early
@@ -138,15 +157,3 @@ def tune(solver: E.Solver, Y_sample, deltaT: float, dtc0: float = 1e-7, deltaT_c
         except Exception:
             pass
     return res
-
-
-def _ws_doubles(mech: E.Mechanism) -> int:
-    """Per-cell workspace in doubles (mirrors make_layout in gf_device.cuh)."""
-    nS = mech.n_species
-    m = nS + 1
-    ld = m | 1
-    slots = 0
-    for r in mech.raw.reactions:
-        slots += 2 + len(r.lhs) + len(r.rhs) + (1 if r.rate_type == 1 else 0)
-    n_tb = sum(1 for r in mech.raw.reactions if r.rate_type != 0)
-    return m * ld + 12 * m + 5 * nS + max(slots, 1) + max(n_tb, 1) + 8

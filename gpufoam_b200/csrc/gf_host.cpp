@@ -680,6 +680,14 @@ int gf_solver_set_launch(gf_solver* s, const gf_launch_config* cfg) {
     return GF_OK;
 }
 
+int gf_solver_info(const gf_solver* s, int* ws_doubles_per_cell, int* max_neq, int* n_mechs) {
+    if (!s) return GF_ERR_INVALID_ARGUMENT;
+    if (ws_doubles_per_cell) *ws_doubles_per_cell = s->max_ws_doubles;
+    if (max_neq) *max_neq = s->max_neq;
+    if (n_mechs) *n_mechs = (int)s->mechs.size();
+    return GF_OK;
+}
+
 int gf_solver_get_launch(const gf_solver* s, gf_launch_config* cfg) {
     if (!s || !cfg) return GF_ERR_INVALID_ARGUMENT;
     *cfg = s->cfg;

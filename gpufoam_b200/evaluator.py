@@ -254,6 +254,12 @@ class Solver:
                                register_budget)
         N.check(self.lib.gf_solver_set_launch(self.handle, C.byref(cfg)), "gf_solver_set_launch")
 
+    def workspace_doubles(self) -> int:
+        """Per-cell workspace of the solve kernels, in doubles (gf_solver_info)."""
+        ws = C.c_int()
+        N.check(self.lib.gf_solver_info(self.handle, C.byref(ws), None, None), "gf_solver_info")
+        return ws.value
+
     def get_launch(self) -> dict:
         cfg = N.GfLaunchConfig()
         N.check(self.lib.gf_solver_get_launch(self.handle, C.byref(cfg)), "gf_solver_get_launch")

@@ -189,6 +189,10 @@ int gf_solver_create(const gf_mech* const* mechs, int n_mechs, const gf_ode_inpu
 void gf_solver_destroy(gf_solver* solver);
 int gf_solver_set_launch(gf_solver* solver, const gf_launch_config* cfg);
 int gf_solver_get_launch(const gf_solver* solver, gf_launch_config* cfg);
+/* The per-cell workspace of the solve kernels (doubles: in shared memory or
+ * HBM, by the launch form), the widest state row (nEqns) and the number of
+ * mechanisms; any output may be NULL. */
+int gf_solver_info(const gf_solver* solver, int* ws_doubles_per_cell, int* max_neq, int* n_mechs);
 
 /* ---- the per-flow-step solve --------------------------------------------- */
 

@@ -4,9 +4,12 @@
 // gpuKernelEvaluator.H:18-85): computeYNew (gpuKernelEvaluator.cu:35-63) and
 // computeRR (gpuKernelEvaluator.cu:65-97) on host vectors; the mechanism comes
 // in as the C ABI's flat structs (gf_thermo with coefficients x R,
-// gf_reaction with its reaction thermo), which the plugin's loaders fill.
-// Errors become std::runtime_error with the library's message; an unknown
-// solver name throws as make_gpuODESolver does (makeGpuOdeSolver.H:28).
+// gf_reaction with its reaction thermo), which the plugin's loaders fill. The
+// ODE inputs come in as the reference's own gpuODESolverInputs
+// (gpuOde/gpuODESolverInputs.H:9-23, the struct read_gpuODESolverInputs
+// returns: any struct with its members name, absTol, ... is accepted) or as a
+// gf_ode_inputs. Errors become std::runtime_error with the library's message;
+// an unknown solver name throws as make_gpuODESolver does (makeGpuOdeSolver.H:28).
 #ifndef GPUFOAM_B200_HPP
 #define GPUFOAM_B200_HPP
 
@@ -48,6 +51,19 @@ inline gf_ode_inputs make_gf_ode_inputs(const std::string& name, double absTol, 
 
 class GpuKernelEvaluator {
 public:
+    GpuKernelEvaluator() = default;
+
+    // The reference's constructor with its gpuODESolverInputs (solver by name).
+    template <class OdeInputs, class = decltype(std::declval<const OdeInputs&>().name.c_str(),
+                                                std::declval<const OdeInputs&>().maxScale)>
+    GpuKernelEvaluator(int nCells, int nEqns, int nSpecie, const std::vector<gf_thermo>& thermos,
+                       const std::vector<gf_reaction>& reactions, const OdeInputs& odeInputs, double Treact = 0.0)
+        : GpuKernelEvaluator(nCells, nEqns, nSpecie, thermos, reactions,
+                             make_gf_ode_inputs(odeInputs.name, odeInputs.absTol, odeInputs.relTol,
+                                                int(odeInputs.maxSteps), odeInputs.safeScale, odeInputs.alphaInc,
+                                                odeInputs.alphaDec, odeInputs.minScale, odeInputs.maxScale),
+                             Treact) {}
+
     GpuKernelEvaluator(int nCells, int nEqns, int nSpecie, const std::vector<gf_thermo>& thermos,
                        const std::vector<gf_reaction>& reactions, const gf_ode_inputs& odeInputs,
                        double Treact = 0.0)
@@ -127,7 +143,7 @@ private:
             throw std::runtime_error("gpufoam_b200: " + msg);
         }
     }
-    int nCells_, nEqns_, nSpecie_;
+    int nCells_ = 0, nEqns_ = 0, nSpecie_ = 0;
     gf_mech* mech_ = nullptr;
     gf_solver* solver_ = nullptr;
 };

@@ -944,6 +944,25 @@ void orc_attempt(void* h, const orc_ode_inputs* o, int nst, const double* y0, co
     ws_free(&w);
 }
 
+/* The frozen-step replay of a recorded integration (the map the adjoint
+ * differentiates): y_{k+1} = attempt(y_k, f(y_k), h_k) for k < n_steps, each
+ * step adaptiveSolve's derivatives call (gpuAdaptiveSolver.H:96) and one
+ * attempt with the recorded size, then singleCellSolver's max(0, Y)
+ * (singleCellSolver.H:41-45). y [nS + 2] in place. */
+void orc_replay(void* h, const orc_ode_inputs* o, int n_steps, const double* steps, double* y) {
+    const mech_t* m = (const mech_t*)h;
+    const int n = m->nS + 2;
+    ws_t w;
+    ws_init(&w, m->nS);
+    for (int k = 0; k < n_steps; ++k) {
+        derivatives(m, &w, y, w.dydx0);
+        attempt(m, &w, o, y, w.dydx0, steps[k], w.yTemp);
+        for (int i = 0; i < n; ++i) y[i] = w.yTemp[i];
+    }
+    for (int i = 0; i < m->nS; ++i) y[i] = fmax(0.0, y[i]);
+    ws_free(&w);
+}
+
 /* adaptiveSolve, gpuAdaptiveSolver.H:83-134. Returns 0, or CELL_STEP_UNDERFLOW
  * where the reference prints and asserts (:111-114). */
 static int adaptive_solve(const mech_t* m, ws_t* w, const orc_ode_inputs* o, double* x, double* y, double* dxTry,

@@ -48,6 +48,7 @@ void orc_jacobian(void* h, int n, const double* y, double* dfdx, double* J);
 void orc_lu(int m, int n_mats, double* A, int* piv, double* b);
 void orc_attempt(void* h, const orc_ode_inputs* o, int n, const double* y0, const double* dydx0,
                  const double* dx, double* y, double* err);
+void orc_replay(void* h, const orc_ode_inputs* o, int n_steps, const double* steps, double* y);
 void orc_cells(void* h, const orc_ode_inputs* o, double Treact, int n, double deltaT,
                const double* deltaT_cell, double* Y, double* deltaTChem, int* counts,
                int* status, int nthreads);

@@ -129,6 +129,7 @@ class Oracle:
         getattr(L, p + "qdot").argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         if kind == "port":
             L.orc_rate_parts.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
+            L.orc_replay.argtypes = [C.c_void_p, C.POINTER(OdeInputs), C.c_int, _dp, _dp]
         self.mech = mech
         fl = flatten(mech)
         self._flat = fl
@@ -220,6 +221,14 @@ class Oracle:
         dtc = np.array(np.broadcast_to(np.asarray(deltaTChem, dtype=np.float64), (n,)), order="C", copy=True)
         self.lib.ref_cells(self.h, C.byref(inputs), Treact, n, float(deltaT), Y, dtc, nthreads)
         return Y, dtc
+
+    def replay(self, inputs: OdeInputs, y0, steps):
+        """The frozen-step map (port only): the recorded step sizes replayed from
+        y0, one attempt each, then max(0, Y)."""
+        y = np.array(y0, dtype=np.float64, order="C", copy=True)
+        st = np.ascontiguousarray(steps, dtype=np.float64)
+        self.lib.orc_replay(self.h, C.byref(inputs), int(st.size), st, y)
+        return y
 
     def compute_rr_host(self, deltaT, deltaTChemMax, rho, Y0, Ynew, deltaTChemNew):
         n = Y0.shape[0]

@@ -2,7 +2,8 @@
 
 The oracle (oracle/gf_oracle.c, pinned to the reference) replays the recorded
 accepted steps with the step sequence frozen: y_{k+1} = Rosenbrock attempt(y_k,
-f(y_k), h_k), then the final max(0, Y) clip of singleCellSolver. Checks:
+f(y_k), h_k), then the final max(0, Y) clip of singleCellSolver (orc_replay).
+Checks:
 
 * initial state: central differences with a relative step of 1e-6 of that map
   along a random direction (all species, T, every cell), to 1e-5 relative;
@@ -10,30 +11,23 @@ f(y_k), h_k), then the final max(0, Y) clip of singleCellSolver. Checks:
   relative steps 1e-4 and 2e-4, Richardson-extrapolated (a 1e-6 step is below
   the loss's rounding noise for the small parameter gradients), to 1e-5
   relative, or 1e-5 of the largest parameter gradient for the tiny ones;
-* a tangent-linear reference on the CPU: a tangent propagated through the
-  recorded steps by directional derivatives of each step map (central, relative
-  step 1e-7), against the adjoint's gradient along the same direction.
+* a tangent-linear reference on the CPU (oracle/complex_step.py): the frozen
+  map restated in complex arithmetic, whose imaginary part at x + i eps d
+  carries the derivative of every operation along d (the complex-step method,
+  exact to rounding), along a random direction of all initial states and a
+  random direction of all rate parameters, against the adjoint's gradient
+  along the same directions, to 1e-5 relative.
 """
+import concurrent.futures
+
 import numpy as np
 import pytest
 
 from gpufoam_b200 import adjoint as AD
 from gpufoam_b200 import evaluator as E
 from gpufoam_b200 import mechanism as M
+from oracle.complex_step import ComplexStepMap
 from oracle.oracle import Oracle, ode_inputs
-
-
-def step_map(orc, inputs, y, h):
-    dydx = orc.derivatives(y[None])[0]
-    return orc.attempt(inputs, y[None], dydx[None], h)[0][0]
-
-
-def frozen_map(orc, inputs, y0, steps, nS):
-    y = np.array(y0, dtype=np.float64)
-    for h in steps:
-        y = step_map(orc, inputs, y, h)
-    y[:nS] = np.maximum(y[:nS], 0.0)
-    return y
 
 
 def test_parameters_roundtrip():
@@ -48,10 +42,10 @@ class Case:
     """One recorded integration on the GPU, its adjoint, and the oracle's
     frozen-step replay."""
 
-    def __init__(self, raw, n_cells, deltaT, solver, seed):
+    def __init__(self, raw, n_cells, deltaT, solver, seed, T_range=(1000.0, 2500.0)):
         import torch
         self.raw, self.nS, self.n = raw, raw.n_species, n_cells
-        self.cells = M.make_cells(raw, n_cells, seed=seed)
+        self.cells = M.make_cells(raw, n_cells, seed=seed, T_range=T_range)
         sol = AD.AdjointSolver(raw, E.OdeInputs(f"Rosenbrock{solver}", absTol=1e-8, relTol=1e-4), traj_cap=2048)
         Y0 = torch.as_tensor(self.cells, device="cuda")
         dtc = torch.full((n_cells,), 1e-7, dtype=torch.float64, device="cuda")
@@ -71,23 +65,23 @@ class Case:
         cnt = counters.cpu().numpy()
         self.steps = [traj[c, :cnt[c, 0], self.nS + 1] for c in range(n_cells)]
         self.Y1 = Y1.cpu().numpy()
+        self.solver = solver
         self.inp = ode_inputs(solver)
         self.orc = Oracle(raw, "port")
 
     def loss(self, orc, cells):
-        return sum(float(np.dot(self.w[c], frozen_map(orc, self.inp, cells[c], self.steps[c], self.nS)))
-                   for c in range(self.n))
+        return sum(float(np.dot(self.w[c], orc.replay(self.inp, cells[c], self.steps[c]))) for c in range(self.n))
 
     def theta_loss(self, theta):
         return self.loss(Oracle(AD.with_parameters(self.raw, theta), "port"), self.cells)
 
 
-def check_case(case, n_params):
+def check_case(case, n_params, replay_rtol=1e-10):
     nS, cells = case.nS, case.cells
     # the replay reproduces the GPU integration
     for c in range(case.n):
-        yf = frozen_map(case.orc, case.inp, cells[c], case.steps[c], nS)
-        np.testing.assert_allclose(yf, case.Y1[c], rtol=1e-10, atol=1e-14)
+        yf = case.orc.replay(case.inp, cells[c], case.steps[c])
+        np.testing.assert_allclose(yf, case.Y1[c], rtol=replay_rtol, atol=1e-14)
     # initial state, random direction, central FD (relative step 1e-6)
     d = case.rng.standard_normal(cells.shape)
     d[:, nS + 1] = 0.0
@@ -96,30 +90,37 @@ def check_case(case, n_params):
     fd = (case.loss(case.orc, cells + eps * scale * d) - case.loss(case.orc, cells - eps * scale * d)) / (2 * eps)
     ad = float(np.sum(case.Y0bar * scale * d))
     assert abs(ad - fd) <= 1e-5 * abs(fd), ("initial state", ad, fd)
-    # tangent-linear reference along the same direction
-    tl = 0.0
-    for c in range(case.n):
-        y = np.array(cells[c])
-        t = scale[c] * d[c]
-        for h in case.steps[c]:
-            e = 1e-7 * np.linalg.norm(y[:nS + 1]) / max(np.linalg.norm(t[:nS + 1]), 1e-300)
-            t = (step_map(case.orc, case.inp, y + e * t, h) - step_map(case.orc, case.inp, y - e * t, h)) / (2 * e)
-            y = step_map(case.orc, case.inp, y, h)
-        t[:nS] = np.where(y[:nS] > 0.0, t[:nS], 0.0)
-        tl += float(np.dot(case.w[c], t))
-    assert abs(ad - tl) <= 1e-5 * abs(tl), ("tangent-linear", ad, tl)
-    # parameters: Richardson-extrapolated central differences
+    # tangent-linear (complex step) along the same direction, and along a
+    # random direction of all rate parameters
+    cs = ComplexStepMap(case.raw, case.solver)
     th0 = AD.parameters_of(case.raw)
-    picks = {(int(case.rng.integers(case.raw.n_reactions)), int(case.rng.integers(3))) for _ in range(n_params)}
+    tl = sum(float(np.dot(case.w[c], cs.directional(cells[c], case.steps[c], th0, dy=scale[c] * d[c])))
+             for c in range(case.n))
+    assert abs(ad - tl) <= 1e-5 * abs(tl), ("tangent-linear, initial state", ad, tl)
+    dth = case.rng.standard_normal(th0.shape) * np.maximum(np.abs(th0), 1.0)
+    tl = sum(float(np.dot(case.w[c], cs.directional(cells[c], case.steps[c], th0, dtheta=dth)))
+             for c in range(case.n))
+    ad = float(np.sum(case.thb * dth))
+    assert abs(ad - tl) <= 1e-5 * abs(tl), ("tangent-linear, parameters", ad, tl)
+    # parameters: Richardson-extrapolated central differences (the losses in parallel)
+    picks = sorted({(int(case.rng.integers(case.raw.n_reactions)), int(case.rng.integers(3)))
+                    for _ in range(n_params)})
     gmax = np.abs(case.thb).max()
-    for r, k in sorted(picks):
+
+    def fd_param(rk):
+        r, k = rk
+
         def fd_at(hr):
             step = hr * max(abs(th0[r, k]), 1.0)
             tp, tm = th0.copy(), th0.copy()
             tp[r, k] += step
             tm[r, k] -= step
             return (case.theta_loss(tp) - case.theta_loss(tm)) / (2 * step)
-        fd = (4.0 * fd_at(1e-4) - fd_at(2e-4)) / 3.0
+        return (4.0 * fd_at(1e-4) - fd_at(2e-4)) / 3.0
+
+    with concurrent.futures.ThreadPoolExecutor() as ex:
+        fds = list(ex.map(fd_param, picks))
+    for (r, k), fd in zip(picks, fds):
         ad = float(case.thb[r, k])
         assert abs(ad - fd) <= 1e-5 * max(abs(fd), gmax), (r, k, ad, fd, gmax)
 
@@ -140,6 +141,16 @@ def test_adjoint_coverage_mechanism():
 @pytest.mark.gpu
 def test_adjoint_grisize():
     check_case(Case(M.gri_size(0), 2, 1e-6, 34, seed=12), n_params=24)
+
+
+@pytest.mark.gpu
+def test_adjoint_differentiation_workload():
+    """The differentiation workload's configuration: the GRI-size mechanism,
+    T ~ U[1100, 1600] K, deltaT = 1e-4 s (through ignition, ~170 accepted
+    steps per cell), Rosenbrock34; 4 cells, 64 random parameters."""
+    case = Case(M.gri_size(0), 4, 1e-4, 34, seed=4096, T_range=(1100.0, 1600.0))
+    assert min(len(s) for s in case.steps) >= 50
+    check_case(case, n_params=64, replay_rtol=1e-6)
 
 
 @pytest.mark.gpu

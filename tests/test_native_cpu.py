@@ -172,3 +172,25 @@ def test_device_tables_pass_the_bounds_check(lib, name):
     raw = fixture_mech(dict(np.load(os.path.join(GOLDEN, f"{name}.npz"))))
     with pytest.raises(N.GfError, match="GF_ERR_NO_DEVICE"):
         E.Mechanism(raw)
+
+
+def test_autotune_cache_key_follows_the_build(monkeypatch):
+    """A cached launch pick is keyed on the library build: a different build
+    digest gives a different key (no GPU needed: the device name is faked)."""
+    import torch
+    from gpufoam_b200 import autotune
+
+    class FakeMech:
+        n_species, n_reactions = 53, 325
+
+        class raw:
+            name = "gri_size"
+
+    monkeypatch.setattr(torch.cuda, "get_device_name", lambda *a: "B200")
+    ode = E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4)
+    monkeypatch.setattr(autotune, "_BUILD_HASH", "aaaa")
+    k1 = autotune._key([FakeMech()], ode)
+    monkeypatch.setattr(autotune, "_BUILD_HASH", "bbbb")
+    assert autotune._key([FakeMech()], ode) != k1
+    monkeypatch.setattr(autotune, "_BUILD_HASH", None)
+    assert len(autotune.build_hash()) == 16
