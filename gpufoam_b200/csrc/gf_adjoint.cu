@@ -18,10 +18,12 @@
 //     concentration dependence, are differentiated as they stand);
 //   * dfdx = f(y0) (the reference fills dfdx with the derivatives,
 //     gpuODESystem.H:198-281), so its adjoint joins f's at y0.
-// Per-reaction derivatives come from forward-mode dual numbers over the
-// reaction's inputs (its species' concentrations, the third-body
-// concentration, T and the k (or k0) Arrhenius parameters ln|A|, beta, Ta);
-// the mixture, conversion and T-row parts are reversed by hand.
+// Per-reaction derivatives w.r.t. the reaction's inputs (its species'
+// concentrations, the third-body concentration, T and the k (or k0) Arrhenius
+// parameters ln|A|, beta, Ta): closed forms for the omega-only products of
+// Arrhenius and third-body reactions, otherwise rxn_vjp (the concentrations in
+// closed form, T, M and the parameters by 5-direction dual numbers); the
+// mixture, conversion and T-row parts are reversed by hand.
 // The loss gradient w.r.t. the final states comes in as Ybar; out come the
 // gradients w.r.t. the initial states (Y, T) and, summed over the sweep, per
 // reaction w.r.t. (ln|A|, beta, Ta) of its k (k0 for fall-off) rate.
@@ -37,7 +39,7 @@
 
 namespace gf {
 
-constexpr int kAdjK = 2 * kSideInline + 5;  // dual directions: species entries, M, T, ln|A|, beta, Ta
+constexpr int kAdjK = 2 * kSideInline + 5;  // reaction inputs: species entries, M, T, ln|A|, beta, Ta
 constexpr int kSeedM = 2 * kSideInline, kSeedT = kSeedM + 1, kSeedLnA = kSeedM + 2, kSeedBeta = kSeedM + 3,
               kSeedTa = kSeedM + 4;
 
@@ -267,7 +269,8 @@ __device__ void adj_mixture_reverse(const Grp<G>& g, const DevMech& M, const W& 
 
 // Per-reaction reverse: omega_bar from dN/dt adjoints (dn) and, when the
 // Jacobian's raw adjoint (rawb, m x ld) is given, the pullback of its terms;
-// dual evaluation over the reaction's inputs; concentration adjoints to the
+// the derivatives w.r.t. the reaction's inputs (closed form or rxn_vjp);
+// concentration adjoints to the
 // per-entry slots (gq), third-body ones to Mb, T to ms[MS_TB] (summed by the
 // caller), parameters to theta_bar (accumulated).
 template <int G, class W>
@@ -384,31 +387,16 @@ __device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, con
             theta_bar[3 * r + 2] += -gk * invT;
             continue;
         }
-        // dual evaluation
-        using D = Dual<kAdjK>;
-        D c[2 * kSideInline];
+        // the vector-Jacobian product of the reaction's quantities (rxn_vjp)
+        double c[2 * kSideInline];
 #pragma unroll
         for (int e = 0; e < 2 * kSideInline; ++e) {
             const int sd = e / kSideInline, ee = e % kSideInline;
             const bool on = ee < (sd ? R.nr : R.nl);
-            c[e] = on ? dseed<kAdjK>(w[L.c + R.idx[sd][ee]], e) : dconst<kAdjK>(1.0);
+            c[e] = on ? w[L.c + R.idx[sd][ee]] : 1.0;
         }
-        const D Mc = dseed<kAdjK>(R.tb_row >= 0 ? w[L.Mtb + R.tb_row] : 0.0, kSeedM);
-        const D Td = dseed<kAdjK>(T, kSeedT);
-        RxnVals<D> v;
-        rxn_eval(M, q, R, c, Mc, Td, dseed<kAdjK>(R.lnA0, kSeedLnA), dseed<kAdjK>(R.beta0, kSeedBeta),
-                 dseed<kAdjK>(R.Ta0, kSeedTa), v);
         double gr[kAdjK];
-#pragma unroll
-        for (int k = 0; k < kAdjK; ++k) {
-            double h = ob * v.omega.d[k];
-            if (rawb >= 0) {
-#pragma unroll
-                for (int e = 0; e < 2 * kSideInline; ++e) h += gD[e] * v.D[e].d[k];
-                h += gT * v.dwdT.d[k] + gE * v.P.d[k];
-            }
-            gr[k] = h;
-        }
+        rxn_vjp(M, q, R, c, R.tb_row >= 0 ? w[L.Mtb + R.tb_row] : 0.0, T, ob, gD, gT, gE, gr);
 #pragma unroll
         for (int e = 0; e < 2 * kSideInline; ++e) wa[A.gq + q * 2 * kSideInline + e] = gr[e];
         if (R.tb_row >= 0) wa[A.Mb + R.tb_row] = gr[kSeedM];

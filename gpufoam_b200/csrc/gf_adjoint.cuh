@@ -1,7 +1,7 @@
 // Differentiation helpers of the discrete adjoint (gf_adjoint.cu): forward-mode
-// dual numbers and the per-reaction quantities of the chemistry written once
-// for a generic scalar, following the same formulas, in the same order, as the
-// double-precision device code in gf_device.cuh (gpuReaction.H,
+// dual numbers, the rate and thermo expressions for a generic scalar, and the
+// per-reaction vector-Jacobian product, following the same formulas, in the
+// same order, as the double-precision device code in gf_device.cuh (gpuReaction.H,
 // gpuThermo.H, gpuArrheniusReactionRate.H, gpuThirdBodyArrheniusReactionRate.H,
 // gpuFallOffReactionRate.H, gpuTroeFallOffFunction.H of the reference).
 #pragma once
@@ -212,26 +212,82 @@ __device__ __forceinline__ S troe_F_s(const DevMech& M, int q, const S& T, const
     return exp(x4 * kLn10);
 }
 
-// The quantities of reaction q that enter the right-hand side and the
-// Jacobian, as stage_omega / stage_jacobian_params compute them:
-//   omega; D[e]: dCf/dc * kf of lhs entry e (e < kSideInline) and dCr/dc * kr of
-//   rhs entry e (kSideInline + e); dwdT; P = Ak (Cf - Cr/Kc) (third body).
-// Inputs: the concentrations of the reaction's species entries c[e], the
-// third-body concentration Mc, T, and the k (or k0) Arrhenius parameters.
-template <class S>
-struct RxnVals {
-    S omega, dwdT, P;
-    S D[2 * kSideInline];
-};
-
-template <class S>
-__device__ __forceinline__ void rxn_eval(const DevMech& M, int q, const Rxn& R, const S* c, const S& Mc, const S& T,
-                                         const S& lnA0, const S& beta0, const S& Ta0, RxnVals<S>& out) {
-    const S invT = 1.0 / T;
-    const S logT = log(T);
-    const S lx = log(kPstd / (kRR * T));
-    const S l0 = beta0 * logT + lnA0 - Ta0 * invT;
-    S kf, ddT, Ak = T * 0.0;
+// The per-reaction vector-Jacobian product of the sweep. The quantities of
+// reaction q that enter the right-hand side and the Jacobian, as
+// stage_omega / stage_jacobian_params compute them, are omega; D[e] = kf dCf_e
+// (lhs entry e < kSideInline) and kr dCr_e (rhs entry kSideInline + e), dC_e
+// = e_e c_e^(e_e - 1) prod_{i != e} c_i^e_i in the reference's product order;
+// dwdT; P = Ak (Cf - Cr/Kc) (third body). With the caller's weights (ob for
+// omega, gD[e] for D[e], gT for dwdT, gE for P) this writes the gradient of
+//   h = ob omega + sum_e gD[e] D[e] + gT dwdT + gE P
+// w.r.t. the reaction's inputs to gr[]: the species entries (lhs 0 ..
+// kSideInline-1, rhs kSideInline ..), then M, T, ln|A|, beta, Ta.
+//   * M, T and the Arrhenius parameters enter through the rate constants and
+//     the equilibrium constant: one forward-mode pass with those 5 directions
+//     and the concentration products held as plain values; h collapses to
+//     ob omega + wf kf + wr kr + gT dwdT + gE P with wf = sum_j gD[j] dCf_j
+//     and wr = sum_j gD[kSideInline + j] dCr_j, so only a few dual values are
+//     live at once.
+//   * The concentrations enter only through the products C and dC_j: their
+//     derivatives in closed form, with the second derivatives e (e - 1) c^(e - 2).
+constexpr int kVjpK = 5;  // M, T, ln|A|, beta, Ta
+__device__ __forceinline__ void rxn_vjp(const DevMech& M, int q, const Rxn& R, const double* c, double Mc_v,
+                                        double T_v, double ob, const double* gD, double gT, double gE,
+                                        double* gr) {
+    using D = Dual<kVjpK>;
+    const D Mc = dseed<kVjpK>(Mc_v, 0);
+    const D T = dseed<kVjpK>(T_v, 1);
+    const D lnA0 = dseed<kVjpK>(R.lnA0, 2), beta0 = dseed<kVjpK>(R.beta0, 3), Ta0 = dseed<kVjpK>(R.Ta0, 4);
+    // concentration products: p = c^e, q1 = e c^(e-1) (as specie_pow_m1), q2 = e (e-1) c^(e-2)
+    double p[2][kSideInline], q1[2][kSideInline], q2[2][kSideInline], Cs[2] = {1.0, 1.0};
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        const int n = side ? R.nr : R.nl;
+#pragma unroll
+        for (int e = 0; e < kSideInline; ++e) {
+            p[side][e] = 1.0;
+            q1[side][e] = 1.0;
+            q2[side][e] = 0.0;
+            if (e < n) {
+                const double x = c[side * kSideInline + e];
+                const int ie = R.iexp[side][e];
+                const double se = R.sexp[side][e];
+                p[side][e] = specie_pow(x, ie, se);
+                q1[side][e] = se * specie_pow_m1(x, ie, se);
+                if (ie != kNoIntExp)
+                    q2[side][e] = ie == 1 ? 0.0 : se * (se - 1.0) * integer_pow(x, ie - 2);
+                else
+                    q2[side][e] = se * (se - 1.0) * real_pow(x, se - 2.0);
+                Cs[side] *= p[side][e];
+            }
+        }
+    }
+    double dC[2][kSideInline];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        const int n = side ? R.nr : R.nl;
+#pragma unroll
+        for (int j = 0; j < kSideInline; ++j) {
+            double d = 0.0;
+            if (j < n) {
+                d = 1.0;
+#pragma unroll
+                for (int i = 0; i < kSideInline; ++i)
+                    if (i < n) d *= (i == j) ? q1[side][i] : p[side][i];
+            }
+            dC[side][j] = d;
+        }
+    }
+    double wsum[2] = {0.0, 0.0};
+#pragma unroll
+    for (int side = 0; side < 2; ++side)
+#pragma unroll
+        for (int j = 0; j < kSideInline; ++j) wsum[side] += gD[side * kSideInline + j] * dC[side][j];
+    // rate constants and the equilibrium constant over T, M and the parameters
+    const D invT = 1.0 / T;
+    const D logT = log(T);
+    const D l0 = beta0 * logT + lnA0 - Ta0 * invT;
+    D kf, ddT, Ak = dconst<kVjpK>(0.0);
     if (R.type == GF_RATE_ARRHENIUS) {
         Ak = R.sA0 * exp(l0);
         kf = Ak;
@@ -242,80 +298,80 @@ __device__ __forceinline__ void rxn_eval(const DevMech& M, int q, const Rxn& R, 
         ddT = Mc * (Ak * ((beta0 + Ta0 * invT) * invT));
     } else {
         const double b1 = ldg(M.beta1 + q), T1 = ldg(M.Ta1 + q), lA1 = ldg(M.lnA1 + q), s1 = ldg(M.sA1 + q);
-        const S l1 = b1 * logT + lA1 - T1 * invT;
-        const S kInf = s1 * exp(l1);
-        const S Pr = ((R.sA0 * s1) * exp(l0 - l1)) * Mc;
-        const S F = R.type == GF_RATE_TROE_FALLOFF ? troe_F_s(M, q, T, invT, Pr) : T * 0.0 + 1.0;
-        const S temp = (Pr / (1.0 + Pr)) * F;
+        const D l1 = b1 * logT + lA1 - T1 * invT;
+        const D kInf = s1 * exp(l1);
+        const D Pr = ((R.sA0 * s1) * exp(l0 - l1)) * Mc;
+        const D F = R.type == GF_RATE_TROE_FALLOFF ? troe_F_s(M, q, T, invT, Pr) : dconst<kVjpK>(1.0);
+        const D temp = (Pr / (1.0 + Pr)) * F;
         kf = kInf * temp;
         ddT = (kInf * ((b1 + T1 * invT) * invT)) * temp;
     }
-    // sides
-    S Cf = T * 0.0 + 1.0, Cr = T * 0.0 + 1.0;
-    S pw[2][kSideInline], dm[2][kSideInline];
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-        const int n = side ? R.nr : R.nl;
-#pragma unroll
-        for (int e = 0; e < kSideInline; ++e) {
-            pw[side][e] = T * 0.0 + 1.0;
-            dm[side][e] = T * 0.0 + 1.0;
-            if (e < n) {
-                const S& x = c[side * kSideInline + e];
-                pw[side][e] = specie_pow_s(x, R.iexp[side][e], R.sexp[side][e]);
-                dm[side][e] = R.sexp[side][e] * specie_pow_m1_s(x, R.iexp[side][e], R.sexp[side][e]);
-            }
-        }
-    }
-#pragma unroll
-    for (int e = 0; e < kSideInline; ++e)
-        if (e < R.nl) Cf = Cf * pw[0][e];
-    S omega = Cf * kf;
-    S dwdT = Cf * ddT;
-    S invKc = T * 0.0 + 1.0, kr = T * 0.0;
+    const double Cf = Cs[0];
+    const bool tb = R.type == GF_RATE_THIRD_BODY_ARRHENIUS;
+    D h = (ob * Cf + wsum[0]) * kf + (gT * Cf) * ddT;
+    double kr_v = 0.0, invKc_v = 1.0, dkrdT_v = 0.0;
     if (!R.irr) {
-        const Poly7 a = reaction_coeffs_at(M, q, val(T), R.Tcommon);
-        const S Gstd = th_Gstd_s(a, T, logT);
-        const S arg = -R.Y * Gstd * invT * (1.0 / kRR);
-        S lnK = val(arg) < 600 ? arg : T * 0.0 + 0.5 * ::log(kVGreat);
-        if (!R.nm_small) lnK = lnK + R.nm * lx;
-        invKc = exp(-lnK);
-        S dK = (th_S_pstd_s(a, T, logT) + Gstd * invT) * R.Y * invT * (1.0 / kRR);
+        const double Cr = Cs[1];
+        const Poly7 a = reaction_coeffs_at(M, q, T_v, R.Tcommon);
+        const D Gstd = th_Gstd_s(a, T, logT);
+        const D arg = -R.Y * Gstd * invT * (1.0 / kRR);
+        D lnK = arg.v < 600 ? arg : dconst<kVjpK>(0.5 * ::log(kVGreat));
+        if (!R.nm_small) lnK = lnK + R.nm * log(kPstd / (kRR * T));
+        const D invKc = exp(-lnK);
+        D dK = (th_S_pstd_s(a, T, logT) + Gstd * invT) * R.Y * invT * (1.0 / kRR);
         if (!R.nm_small) dK = dK - R.nm * invT;
-        kr = kf * invKc;
-#pragma unroll
-        for (int e = 0; e < kSideInline; ++e)
-            if (e < R.nr) Cr = Cr * pw[1][e];
-        const S dkrdT = ddT * invKc - kr * dK;
-        dwdT = dwdT - Cr * dkrdT;
-        omega = omega - Cr * kr;
-    } else {
-        Cr = T * 0.0;
+        const D kr = kf * invKc;
+        const D dkrdT = ddT * invKc - kr * dK;
+        // omega -= Cr kr, dwdT -= Cr dkrdT, D[rhs] = kr dCr
+        h = h + (wsum[1] - ob * Cr) * kr - (gT * Cr) * dkrdT;
+        if (tb) h = h + gE * (Ak * (Cf - Cr * invKc));
+        kr_v = kr.v;
+        invKc_v = invKc.v;
+        dkrdT_v = dkrdT.v;
+    } else if (tb) {
+        h = h + gE * (Ak * Cf);
     }
+#pragma unroll
+    for (int k = 0; k < kVjpK; ++k) gr[2 * kSideInline + k] = h.d[k];
+    // the species entries, closed form
+    const double kf_v = kf.v, ddT_v = ddT.v, Ak_v = Ak.v;
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
         const int n = side ? R.nr : R.nl;
+        const bool on = !(side && R.irr);
+        const double ks = side ? kr_v : kf_v;
+        // d(ob omega + gT dwdT + gE P) per unit dC_k of this side
+        const double wk = side ? -(ob * kr_v + gT * dkrdT_v + (tb ? gE * Ak_v * invKc_v : 0.0))
+                               : ob * kf_v + gT * ddT_v + (tb ? gE * Ak_v : 0.0);
 #pragma unroll
-        for (int j = 0; j < kSideInline; ++j) {
-            S d = T * 0.0 + 1.0;
-            if (j < n) {
+        for (int k = 0; k < kSideInline; ++k) {
+            double g = 0.0;
+            if (k < n && on) {
+                // sum_j gD[j] d(dC_j)/dc_k
+                double s2 = 0.0;
 #pragma unroll
-                for (int i = 0; i < kSideInline; ++i)
-                    if (i < n) d = d * ((i == j) ? dm[side][i] : pw[side][i]);
-                d = d * (side ? kr : kf);
-            } else {
-                d = T * 0.0;
+                for (int j = 0; j < kSideInline; ++j) {
+                    if (j < n) {
+                        double d = 1.0;
+#pragma unroll
+                        for (int i = 0; i < kSideInline; ++i) {
+                            if (i < n) {
+                                if (i == j && i == k)
+                                    d *= q2[side][i];
+                                else if (i == j || i == k)
+                                    d *= q1[side][i];
+                                else
+                                    d *= p[side][i];
+                            }
+                        }
+                        s2 += gD[side * kSideInline + j] * d;
+                    }
+                }
+                g = wk * dC[side][k] + ks * s2;
             }
-            out.D[side * kSideInline + j] = d;
+            gr[side * kSideInline + k] = g;
         }
     }
-    if (R.irr) {
-#pragma unroll
-        for (int j = 0; j < kSideInline; ++j) out.D[kSideInline + j] = T * 0.0;
-    }
-    out.omega = omega;
-    out.dwdT = dwdT;
-    out.P = R.type == GF_RATE_THIRD_BODY_ARRHENIUS ? Ak * (Cf - Cr * invKc) : T * 0.0;
 }
 
 }  // namespace gf
