@@ -70,7 +70,8 @@ class GfOdeInputs(C.Structure):
 
 class GfLaunchConfig(C.Structure):
     _fields_ = [("kind", C.c_int), ("threads_per_cell", C.c_int), ("scratch_in_shared", C.c_int),
-                ("cells_per_block", C.c_int), ("blocks_per_sm", C.c_int), ("register_budget", C.c_int)]
+                ("cells_per_block", C.c_int), ("blocks_per_sm", C.c_int), ("register_budget", C.c_int),
+                ("lu_panel", C.c_int), ("specialize", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -1504,10 +1504,10 @@ __device__ __forceinline__ void lu_solve_any(const Grp<G>& g, const W& w, int A,
 
 // The factorisation as the solve kernels run it, after the row scaling vv:
 // the register-panel form for a full warp or a multi-warp group (m <= 64),
-// the blocked form otherwise; then, for groups of 16 or more threads, the
+// the blocked form otherwise, both with panels of NB columns; then, for groups of 16 or more threads, the
 // reciprocal pivots 1 / U[i][i] (written over vv, which is no longer needed)
 // and the row permutation of the solves (lu_solve_any).
-template <int G, bool EXACT = false, class W>
+template <int G, bool EXACT = false, int NB = 8, class W>
 __device__ __forceinline__ void lu_factor(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv, int perm,
                                           int m) {
     {
@@ -1515,11 +1515,11 @@ __device__ __forceinline__ void lu_factor(const Grp<G>& g, const W& w, int A, in
         bool done = false;
         if constexpr (G >= 32) {
             if (m <= 64) {
-                lu_decompose_regpanel<G, 8, EXACT>(g, w, A, ld, piv, vv, m);
+                lu_decompose_regpanel<G, NB, EXACT>(g, w, A, ld, piv, vv, m);
                 done = true;
             }
         }
-        if (!done) lu_decompose_blocked<G, 8, EXACT>(g, w, A, ld, piv, vv, m);
+        if (!done) lu_decompose_blocked<G, NB, EXACT>(g, w, A, ld, piv, vv, m);
         GF_PH_END(g, PH_LU)
     }
     if (G >= 16) {
@@ -1611,7 +1611,7 @@ __device__ __forceinline__ double ros_d(const RosCoeffs& C, int i) {
 }
 
 // I/(gamma dx) - J of the Jacobian in L.J, and its LU (gpuAdaptiveSolver.H:51-73).
-template <int G, class W>
+template <int G, class W, int NB = 8>
 __device__ __forceinline__ void shift_and_factor(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
                                                  const RosCoeffs& C, double dx) {
     const int m = M.m;
@@ -1621,15 +1621,15 @@ __device__ __forceinline__ void shift_and_factor(const Grp<G>& g, const DevMech&
         shift_and_scale(g, w, L.J, ld, L.vv, m, 1.0 / (C.gamma * dx));
         GF_PH_END(g, PH_SHIFT)
     }
-    lu_factor(g, w, L.J, ld, L.piv, L.vv, L.perm, m);
+    lu_factor<G, false, NB>(g, w, L.J, ld, L.piv, L.vv, L.perm, m);
 }
 
 // The Jacobian at y0, then shift_and_factor.
-template <int G, class W>
+template <int G, class W, int NB = 8>
 __device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
                                             const RosCoeffs& C, int y0_off, double p, double dx) {
     jacobian(g, M, w, L, y0_off, p, true);
-    shift_and_factor(g, M, w, L, C, dx);
+    shift_and_factor<G, W, NB>(g, M, w, L, C, dx);
 }
 
 // One attempt solve(y0, dydx0, dx, y) of gpuRosenbrock12/23/34 (their
@@ -1643,13 +1643,13 @@ __device__ __forceinline__ void factor_step(const Grp<G>& g, const DevMech& M, c
 // dydx0 when first_deriv is set (the first attempt of a step), through the
 // stage loop's derivative call: one call site, a smaller instruction
 // footprint. Otherwise the caller provides dydx0.
-template <int G, class W, bool SAVE = false, bool F0 = false>
+template <int G, class W, bool SAVE = false, bool F0 = false, int NB = 8>
 __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const RosCoeffs& C,
                               const OdeParams& o, int y0_off, int yt_off, double p, double dx, int save_y2 = -1,
                               int save_y3 = -1, bool first_deriv = false, int save_f2 = -1, int save_f3 = -1) {
     const int m = M.m;
     const int ld = L.ld;
-    if constexpr (!F0 && !SAVE) factor_step(g, M, w, L, C, y0_off, p, dx);
+    if constexpr (!F0 && !SAVE) factor_step<G, W, NB>(g, M, w, L, C, y0_off, p, dx);
     // stages: k_i solves (I/(gamma dx) - J) k_i = f_i + dx d_i dfdx + sum_j c_ij k_j / dx,
     // f_0 = f(y0), f_i = f(y0 + sum_j a_ij k_j) where the method takes a new
     // derivative (stage 1; stage 2 of Rosenbrock34), else the previous one.
@@ -1679,7 +1679,7 @@ __device__ __forceinline__ double ros_attempt(const Grp<G>& g, const DevMech& M,
         }
         if constexpr (F0) {
             if (st < 0) {
-                factor_step(g, M, w, L, C, y0_off, p, dx);
+                factor_step<G, W, NB>(g, M, w, L, C, y0_off, p, dx);
                 continue;
             }
         }
@@ -1735,7 +1735,7 @@ struct CellResult {
 // returns without writing it).
 // REC (the adjoint's forward pass): each accepted step's start state and
 // size are recorded at rec (rec_cap steps at most, rec_ld doubles each).
-template <int G, class W, bool REC = false>
+template <int G, class W, bool REC = false, int NB = 8>
 __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L, const OdeParams& o,
                          const RosCoeffs& C, double xStart, double xEnd, int* y_off, int* yt_off, double p,
                          double* dxTry, int* accepted, int* attempts, double* rec = nullptr, int rec_cap = 0,
@@ -1758,7 +1758,7 @@ __device__ __forceinline__ int ode_solve(const Grp<G>& g, const DevMech& M, cons
         if constexpr (REC) derivatives(g, M, w, L, *y_off, p, L.dydx0, true);
         do {
             GF_PH_BEGIN(g)
-            err = ros_attempt<G, W, false, !REC>(g, M, w, L, C, o, *y_off, *yt_off, p, dx, -1, -1, rejects == 0);
+            err = ros_attempt<G, W, false, !REC, NB>(g, M, w, L, C, o, *y_off, *yt_off, p, dx, -1, -1, rejects == 0);
             GF_PH_END(g, PH_ATTEMPT)
             ++*attempts;
             if (err > 1) {
@@ -1804,8 +1804,9 @@ __device__ __forceinline__ unsigned long long dbl_key(double v) {
 // singleCellSolver::operator() (singleCellSolver.H:27-51) with the
 // computeYNew / computeRR epilogue (gpuKernelEvaluator.cu:84-96) fused:
 // RR, the min of deltaTChemNew before clamping, and the clamp.
-template <int G, class W, bool REC = false>
-__device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, const W& w, const LaunchArgs& a, int cell) {
+template <int G, class W, bool REC = false, int NB = 8>
+__device__ __forceinline__ void process_cell_body(const Grp<G>& g, const DevMech& M, const W& w, const LaunchArgs& a,
+                                                  int cell) {
     const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
     const int nS = M.nS, m = M.m;
     const double* yin = a.Y0 + (size_t)cell * a.ld_y;
@@ -1824,7 +1825,7 @@ __device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, 
         while (timeLeft > kSmall) {
             const double dt = timeLeft;
             double* rec = REC ? a.traj + (size_t)cell * a.traj_cap * a.traj_ld : nullptr;
-            const int st = ode_solve<G, W, REC>(g, M, w, L, a.ode, C, 0.0, dt, &y_off, &yt_off, p, &dxTry, &accepted,
+            const int st = ode_solve<G, W, REC, NB>(g, M, w, L, a.ode, C, 0.0, dt, &y_off, &yt_off, p, &dxTry, &accepted,
                                                 &attempts, rec, a.traj_cap, a.traj_ld);
             if (st != GF_CELL_OK && status == GF_CELL_OK) status = st;
             if (st == GF_CELL_STEP_UNDERFLOW) break;
@@ -1869,6 +1870,23 @@ __device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, 
         if (status != GF_CELL_OK && status != GF_CELL_SKIPPED) atomicAdd(a.queue + 4, 1ull);
     }
     g.sync();
+}
+
+// process_cell_body with the LU panel width NB and, for MS > 0, the matrix
+// size m = MS (nS = MS - 1) fixed at compile time: the caller launches such a
+// kernel only for mechanisms of that size, and the compiler then resolves the
+// workspace offsets, loop bounds and tile predicates that depend on it.
+template <int G, class W, bool REC = false, int NB = 8, int MS = 0>
+__device__ __forceinline__ void process_cell(const Grp<G>& g, const DevMech& M, const W& w, const LaunchArgs& a,
+                                             int cell) {
+    if constexpr (MS == 0) {
+        process_cell_body<G, W, REC, NB>(g, M, w, a, cell);
+    } else {
+        DevMech Ms = M;
+        Ms.m = MS;
+        Ms.nS = MS - 1;
+        process_cell_body<G, W, REC, NB>(g, Ms, w, a, cell);
+    }
 }
 
 }  // namespace gf

@@ -638,7 +638,7 @@ int gf_solver_create(const gf_mech* const* mechs, int n_mechs, const gf_ode_inpu
     // default launch: persistent, two warps per cell (one cell per CTA),
     // workspace in shared memory when it fits (the autotuner refines this per
     // mechanism)
-    s->cfg = gf_launch_config{1, 64, 1, 1, 0, 0};  // kind, G, shared, cells/CTA, CTAs/SM, registers
+    s->cfg = gf_launch_config{1, 64, 1, 1, 0, 0, 0, 0};  // kind, G, shared, cells/CTA, CTAs/SM, registers, panel, specialize
     if ((size_t)s->max_ws_doubles * sizeof(double) > 227 * 1024) s->cfg.scratch_in_shared = 0;
     cudaError_t e = cudaMalloc(&s->queue, 8 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&s->queue_host, 8 * sizeof(unsigned long long));
@@ -675,6 +675,20 @@ int gf_solver_set_launch(gf_solver* s, const gf_launch_config* cfg) {
         if (cfg->register_budget != 0 && cfg->register_budget != 1) return GF_ERR_INVALID_ARGUMENT;
         if (cfg->scratch_in_shared && (size_t)s->max_ws_doubles * sizeof(double) > 227 * 1024)
             return GF_ERR_UNSUPPORTED;
+        if (cfg->lu_panel != 0 && cfg->lu_panel != 4 && cfg->lu_panel != 8 && cfg->lu_panel != 16)
+            return GF_ERR_INVALID_ARGUMENT;
+        if (cfg->specialize != 0 && cfg->specialize != 1) return GF_ERR_INVALID_ARGUMENT;
+        // the tuned variants: 32, 64 and 128 threads, the form's usual register
+        // budget, panels of 4 or 16 columns in shared memory, or a compile-time
+        // matrix size every mechanism of the solver has
+        const bool panel = cfg->lu_panel == 4 || cfg->lu_panel == 16;
+        if (panel || cfg->specialize) {
+            if ((G != 32 && G != 64 && G != 128) || cfg->register_budget != (G == 128 ? 1 : 0))
+                return GF_ERR_UNSUPPORTED;
+            if (panel && (cfg->specialize || !cfg->scratch_in_shared)) return GF_ERR_UNSUPPORTED;
+            if (cfg->specialize && gf::specialized_size(s->dmechs.data(), (int)s->dmechs.size()) == 0)
+                return GF_ERR_UNSUPPORTED;
+        }
     }
     s->cfg = *cfg;
     return GF_OK;
@@ -740,7 +754,8 @@ int solve_slots(const gf_solver* s, int n_cells, int* slots) {
         return GF_OK;
     }
     int blocks = 0, threads = 0;
-    const int k = gf::persistent_slots(s->cfg, s->max_ws_doubles * (int)sizeof(double), &blocks, &threads);
+    const int ms = gf::specialized_size(s->dmechs.data(), (int)s->dmechs.size());
+    const int k = gf::persistent_slots(s->cfg, ms, s->max_ws_doubles * (int)sizeof(double), &blocks, &threads);
     if (k <= 0) return GF_ERR_UNSUPPORTED;
     if (!s->cfg.scratch_in_shared) *slots = k;
     return GF_OK;

@@ -216,7 +216,10 @@ int mech_device(const gf_mech* m);
 int record_cuda_error(int cuda_error);
 
 // Resident-slot count for a persistent configuration (groups that run at once).
-int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* blocks_out, int* threads_out);
+// ms: specialized_size of the launch's mechanisms.
+int persistent_slots(const gf_launch_config& cfg, int ms, int smem_bytes_per_cell, int* blocks_out,
+                     int* threads_out);
+int specialized_size(const DevMech* mechs, int n_mechs);
 int device_sm_count();
 
 }  // namespace gf

@@ -188,7 +188,34 @@ int device_sm_count() {
     return n;
 }
 
-static const void* persistent_fn(int G, bool shared, int slim) {
+// The matrix size the tuned kernels are compiled for when every mechanism of a
+// launch has it (10-, 53- and 100-species mechanisms), else 0.
+int specialized_size(const DevMech* mechs, int n_mechs) {
+    if (n_mechs < 1) return 0;
+    const int m = mechs[0].m;
+    for (int i = 1; i < n_mechs; ++i)
+        if (mechs[i].m != m) return 0;
+    return (m == 11 || m == 54 || m == 101) ? m : 0;
+}
+
+// The persistent kernel of a launch form: the generic variants of every group
+// size, or (lu_panel 4 / 16, or specialize with the matrix size ms) the tuned
+// variants of the 32-, 64- and 128-thread forms; nullptr if not compiled.
+static const void* persistent_fn(const gf_launch_config& cfg, int ms) {
+    const int G = cfg.threads_per_cell;
+    const bool shared = cfg.scratch_in_shared != 0;
+    const int slim = cfg.register_budget;
+    const int nb = (cfg.lu_panel == 0) ? 8 : cfg.lu_panel;
+    const int sms = cfg.specialize ? ms : 0;
+    if (cfg.specialize && sms == 0) return nullptr;
+    if (nb != 8 || sms != 0) {
+        switch (G) {
+        case 32: return persistent_tuned_fn_g32(shared, slim, nb, sms);
+        case 64: return persistent_tuned_fn_g64(shared, slim, nb, sms);
+        case 128: return persistent_tuned_fn_g128(shared, slim, nb, sms);
+        default: return nullptr;
+        }
+    }
     switch (G) {
     case 1: return persistent_fn_g1(shared, slim);
     case 2: return persistent_fn_g2(shared, slim);
@@ -203,10 +230,11 @@ static const void* persistent_fn(int G, bool shared, int slim) {
     }
 }
 
-int persistent_slots(const gf_launch_config& cfg, int smem_bytes_per_cell, int* blocks_out, int* threads_out) {
+int persistent_slots(const gf_launch_config& cfg, int ms, int smem_bytes_per_cell, int* blocks_out,
+                     int* threads_out) {
     const int G = cfg.threads_per_cell;
     const bool shared = cfg.scratch_in_shared != 0;
-    const void* fn = persistent_fn(G, shared, cfg.register_budget);
+    const void* fn = persistent_fn(cfg, ms);
     if (!fn) return -1;
     // G <= 32: several groups per CTA of at most 128 threads; G > 32: one group
     int cpb = G > 32 ? 1 : (cfg.cells_per_block > 0 ? cfg.cells_per_block : std::max(1, 128 / G));
@@ -259,13 +287,14 @@ int launch_cells(const DevMech* mechs, int n_mechs, const gf_launch_config& cfg,
     const int G = cfg.threads_per_cell;
     const bool shared = cfg.scratch_in_shared != 0;
     int blocks = 0, threads = 0;
-    const int slots = persistent_slots(cfg, ws_doubles_per_cell * (int)sizeof(double), &blocks, &threads);
+    const int ms = specialized_size(mechs, n_mechs);
+    const int slots = persistent_slots(cfg, ms, ws_doubles_per_cell * (int)sizeof(double), &blocks, &threads);
     if (slots <= 0) return (int)cudaErrorInvalidConfiguration;
     if (!shared && slots > n_slots_total) return (int)cudaErrorInvalidValue;
     const size_t smem = shared ? (size_t)(threads / G) * ws_doubles_per_cell * sizeof(double) : 0;
     const long long n_slots = slots;
     void* args[] = {(void*)&P, (void*)&a, (void*)&ws_doubles_per_cell, (void*)&n_slots};
-    return (int)cudaLaunchKernel(persistent_fn(G, shared, cfg.register_budget), dim3(blocks), dim3(threads), args,
+    return (int)cudaLaunchKernel(persistent_fn(cfg, ms), dim3(blocks), dim3(threads), args,
                                  smem, s);
 }
 

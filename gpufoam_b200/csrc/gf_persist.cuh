@@ -60,7 +60,9 @@ struct PersistShape {
     static constexpr int kMinBlocksSlim = 512 / kThreads;
 };
 
-template <int G, bool SHARED, int SLIM>
+// NB: columns per LU panel; MS > 0: the matrix size m of every mechanism of
+// the launch, fixed at compile time (process_cell).
+template <int G, bool SHARED, int SLIM, int NB = 8, int MS = 0>
 __global__ void __launch_bounds__(PersistShape<G>::kThreads, SLIM ? PersistShape<G>::kMinBlocksSlim : 1)
     persistent_kernel(const MechSet P, const LaunchArgs a, int ws_per_cell, long long n_slots) {
     extern __shared__ double smem[];
@@ -80,22 +82,51 @@ __global__ void __launch_bounds__(PersistShape<G>::kThreads, SLIM ? PersistShape
         }
         const DevMech& M = *Mp;
         if (SHARED) {
-            process_cell(g, M, WsC{smem + (size_t)gib * ws_per_cell}, a, (int)cell);
+            process_cell<G, WsC, false, NB, MS>(g, M, WsC{smem + (size_t)gib * ws_per_cell}, a, (int)cell);
         } else if (G == 1) {
-            process_cell(g, M, WsS{a.ws + slot, n_slots}, a, (int)cell);
+            process_cell<G, WsS, false, NB, MS>(g, M, WsS{a.ws + slot, n_slots}, a, (int)cell);
         } else {
-            process_cell(g, M, WsC{a.ws + slot * ws_per_cell}, a, (int)cell);
+            process_cell<G, WsC, false, NB, MS>(g, M, WsC{a.ws + slot * ws_per_cell}, a, (int)cell);
         }
     }
 }
 
-template <int G>
+template <int G, int NB = 8, int MS = 0>
 const void* persistent_variant(bool shared, int slim) {
     if (shared)
-        return slim ? reinterpret_cast<const void*>(&persistent_kernel<G, true, 1>)
-                    : reinterpret_cast<const void*>(&persistent_kernel<G, true, 0>);
-    return slim ? reinterpret_cast<const void*>(&persistent_kernel<G, false, 1>)
-                : reinterpret_cast<const void*>(&persistent_kernel<G, false, 0>);
+        return slim ? reinterpret_cast<const void*>(&persistent_kernel<G, true, 1, NB, MS>)
+                    : reinterpret_cast<const void*>(&persistent_kernel<G, true, 0, NB, MS>);
+    return slim ? reinterpret_cast<const void*>(&persistent_kernel<G, false, 1, NB, MS>)
+                : reinterpret_cast<const void*>(&persistent_kernel<G, false, 0, NB, MS>);
+}
+
+// The tuned variants of the 32-, 64- and 128-thread forms (gf_persist_g<G>_tuned.cu):
+// LU panels of 4 or 16 columns (workspace in shared memory), and the matrix
+// size fixed at compile time for the 10-, 53- and 100-species mechanisms
+// (m = 11, 54, 101; workspace in shared memory or HBM). Each with the register
+// budget the form is usually run with (SLIM for 128 threads); nullptr for a
+// variant that is not compiled.
+constexpr int kTunedSlim(int G) { return G == 128 ? 1 : 0; }
+template <int G>
+const void* persistent_tuned_variant(bool shared, int slim, int nb, int ms) {
+    if (slim != kTunedSlim(G)) return nullptr;
+    constexpr int S = kTunedSlim(G);
+    if (ms == 0) {
+        if (!shared) return nullptr;
+        if (nb == 4) return reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 4, 0>);
+        if (nb == 16) return reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 16, 0>);
+        return nullptr;
+    }
+    if (nb != 8) return nullptr;
+    switch (ms) {
+    case 11: return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 8, 11>)
+                           : reinterpret_cast<const void*>(&persistent_kernel<G, false, S, 8, 11>);
+    case 54: return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 8, 54>)
+                           : reinterpret_cast<const void*>(&persistent_kernel<G, false, S, 8, 54>);
+    case 101: return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 8, 101>)
+                            : reinterpret_cast<const void*>(&persistent_kernel<G, false, S, 8, 101>);
+    default: return nullptr;
+    }
 }
 
 // defined in gf_persist_g<G>.cu
@@ -108,6 +139,10 @@ const void* persistent_fn_g32(bool shared, int slim);
 const void* persistent_fn_g64(bool shared, int slim);
 const void* persistent_fn_g128(bool shared, int slim);
 const void* persistent_fn_g256(bool shared, int slim);
+// defined in gf_persist_g<G>_tuned.cu
+const void* persistent_tuned_fn_g32(bool shared, int slim, int nb, int ms);
+const void* persistent_tuned_fn_g64(bool shared, int slim, int nb, int ms);
+const void* persistent_tuned_fn_g128(bool shared, int slim, int nb, int ms);
 
 #ifdef GF_PHASE_TIMERS
 // phase-timer accumulators of the gf_persist_g<G>.cu units (profiling builds)

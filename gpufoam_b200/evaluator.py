@@ -249,9 +249,9 @@ class Solver:
         self.max_species = max(m.n_species for m in self.mechs)
 
     def set_launch(self, kind=1, threads_per_cell=32, scratch_in_shared=1, cells_per_block=0, blocks_per_sm=0,
-                   register_budget=0):
+                   register_budget=0, lu_panel=0, specialize=0):
         cfg = N.GfLaunchConfig(kind, threads_per_cell, scratch_in_shared, cells_per_block, blocks_per_sm,
-                               register_budget)
+                               register_budget, lu_panel, specialize)
         N.check(self.lib.gf_solver_set_launch(self.handle, C.byref(cfg)), "gf_solver_set_launch")
 
     def workspace_doubles(self) -> int:

@@ -37,3 +37,47 @@ def test_tuned_form_passes_parity():
     assert (out["status"].cpu().numpy() == 0).all()
     assert_states_close(out["Ynew"].cpu().numpy(), ref[0], raw.n_species, 1e-4, f"tuned form {best}")
     assert step_count_agreement(out["counters"].cpu().numpy(), ref[2]) >= 0.99
+
+
+@pytest.mark.parametrize("factory", [M.h2_size, M.gri_size, M.large])
+def test_tuned_variants_parity(factory):
+    """Every tile and specialisation variant the autotuner can pick (LU panels
+    of 4 and 16 columns; the kernel compiled for the mechanism's matrix size,
+    m = 11, 54, 101) against the oracle, for 32, 64 and 128 threads per cell."""
+    import torch
+    from gpufoam_b200 import _native as N
+    raw = factory(0)
+    mech = E.Mechanism(raw)
+    ode = E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4)
+    n = 64
+    cells = M.make_cells(raw, n, seed=73)
+    dT = 1e-5 if raw.n_species <= 10 else 1e-6
+    ref = Oracle(raw, "port").cells(ode_inputs(34), cells, dT, 1e-7)
+    ws = E.Solver([mech], ode).workspace_doubles() * 8
+    for G in (32, 64, 128):
+        regs = 1 if G == 128 else 0
+        forms = [dict(specialize=1, scratch_in_shared=0)]
+        if ws <= 227 * 1024:
+            forms += [dict(specialize=1, scratch_in_shared=1), dict(lu_panel=4, scratch_in_shared=1),
+                      dict(lu_panel=16, scratch_in_shared=1)]
+        for f in forms:
+            s = E.Solver([mech], ode)
+            s.set_launch(kind=1, threads_per_cell=G, register_budget=regs, **f)
+            dtc = torch.full((n,), 1e-7, dtype=torch.float64, device="cuda")
+            out = s.solve(torch.as_tensor(cells, device="cuda"), dT, dtc)
+            torch.cuda.synchronize()
+            st = out["status"].cpu().numpy()
+            assert np.array_equal(st, ref[3]), (G, f)
+            ok = st == 0
+            assert_states_close(out["Ynew"].cpu().numpy()[ok], ref[0][ok], raw.n_species, 1e-4, f"G={G} {f}")
+            assert step_count_agreement(out["counters"].cpu().numpy(), ref[2]) >= 0.99
+    # forms that are not compiled are refused
+    s = E.Solver([mech], ode)
+    for bad in (dict(threads_per_cell=16, specialize=1), dict(threads_per_cell=64, register_budget=1, lu_panel=4),
+                dict(threads_per_cell=64, lu_panel=4, scratch_in_shared=0),
+                dict(threads_per_cell=64, lu_panel=16, specialize=1)):
+        with pytest.raises(N.GfError, match="UNSUPPORTED"):
+            s.set_launch(kind=1, **bad)
+    cov = E.Mechanism(M.coverage(0))   # 12 species: no kernel compiled for m = 13
+    with pytest.raises(N.GfError, match="UNSUPPORTED"):
+        E.Solver([cov], ode).set_launch(kind=1, threads_per_cell=64, specialize=1)
