@@ -692,7 +692,7 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
 __global__ void __launch_bounds__(64) adjoint_kernel(const DevMech M, const AdjArgs a) {
     extern __shared__ double smem[];
     Grp<64> g;
-    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
+    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb, true);
     int fwd = 0;
     const AdjLayout A = make_adj_layout(L, M.nS, M.nR, M.n_tb, &fwd);
     WsC w{smem};
@@ -767,13 +767,13 @@ int launch_record(const DevMech& M, const LaunchArgs& a, void* stream) {
 }
 
 int adjoint_ws_doubles(const DevMech& M) {
-    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
+    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb, true);
     int fwd = 0;
     return make_adj_layout(L, M.nS, M.nR, M.n_tb, &fwd).size;
 }
 
 static int adjoint_smem_bytes(const DevMech& M) {
-    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
+    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb, true);
     int fwd = 0;
     make_adj_layout(L, M.nS, M.nR, M.n_tb, &fwd);
     return fwd * (int)sizeof(double);

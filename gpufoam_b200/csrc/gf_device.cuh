@@ -480,7 +480,13 @@ __device__ __forceinline__ double rate_k(const DevMech& M, int q, const Rxn& R, 
 
 // ------------------------------------------------------------- layout
 
-__host__ __device__ inline WsLayout make_layout(int nS, int nR, int n_slots, int n_tb) {
+// Per-cell workspace layout. The solve kernels (sweep = false) keep Cp, v and
+// rhoM/W, which only the Jacobian reads, in k2..k4 (the stage vectors, not yet
+// written while the Jacobian is built), and have one pivot region: the solves
+// follow either the pivots or their permutation (solve_layout places the other
+// in k1, free until the first stage). The adjoint's sweep (sweep = true) needs
+// both after the stages and gets separate regions.
+__host__ __device__ inline WsLayout make_layout(int nS, int nR, int n_slots, int n_tb, bool sweep = false) {
     WsLayout L;
     const int m = nS + 1;
     L.ld = m | 1;
@@ -498,12 +504,22 @@ __host__ __device__ inline WsLayout make_layout(int nS, int nR, int n_slots, int
     L.k4 = o; o += m;
     L.vv = o; o += m;
     L.piv = o; o += m;
-    L.perm = o; o += m;
+    if (sweep) {
+        L.perm = o; o += m;
+    } else {
+        L.perm = L.piv;
+    }
     L.c = o; o += nS;
-    L.Cp = o; o += nS;
     L.Ha = o; o += nS;
-    L.rhoMbyW = o; o += nS;
-    L.vj = o; o += nS;
+    if (sweep) {
+        L.Cp = o; o += nS;
+        L.rhoMbyW = o; o += nS;
+        L.vj = o; o += nS;
+    } else {
+        L.Cp = L.k2;
+        L.vj = L.k3;
+        L.rhoMbyW = L.k4;
+    }
     L.stage = o; o += (n_slots > 0 ? n_slots : 1);
     L.Mtb = o; o += (n_tb > 0 ? n_tb : 1);
     L.scal = o; o += 8;
@@ -1371,6 +1387,26 @@ __device__ __forceinline__ void lu_perm(const Grp<G>& g, const W& w, int piv, in
 // reciprocal of the diagonal, rdiag[j] = 1 / U[j][j] (computed once per LU),
 // instead of dividing (ulp-level).
 constexpr int kRegRows = 160;
+
+// Whether the solves of a group of G threads (lu_solve_any) take the row
+// permutation as a gather list (perm) or follow the pivots step by step (piv).
+template <int G>
+__host__ __device__ constexpr bool solve_uses_perm(int m) {
+    return (G >= 32 && m <= 64) || (G >= 16 && G <= 32 && m <= kRegRows);
+}
+
+// The solve kernels' layout for a group of G threads: the pivot array the
+// solves do not read (written by the factorisation or by lu_perm, consumed
+// before the first stage) goes to k1.
+template <int G>
+__host__ __device__ inline WsLayout solve_layout(int nS, int nR, int n_slots, int n_tb) {
+    WsLayout L = make_layout(nS, nR, n_slots, n_tb);
+    if (solve_uses_perm<G>(nS + 1))
+        L.piv = L.k1;
+    else
+        L.perm = L.k1;
+    return L;
+}
 template <int G, class W>
 __device__ __forceinline__ void lu_solve_reg(const Grp<G>& g, const W& w, int A, int ld, int perm, int rdiag, int m,
                                              int b) {
@@ -1807,7 +1843,7 @@ __device__ __forceinline__ unsigned long long dbl_key(double v) {
 template <int G, class W, bool REC = false, int NB = 8>
 __device__ __forceinline__ void process_cell_body(const Grp<G>& g, const DevMech& M, const W& w, const LaunchArgs& a,
                                                   int cell) {
-    const WsLayout L = make_layout(M.nS, M.nR, M.n_slots, M.n_tb);
+    const WsLayout L = solve_layout<G>(M.nS, M.nR, M.n_slots, M.n_tb);
     const int nS = M.nS, m = M.m;
     const double* yin = a.Y0 + (size_t)cell * a.ld_y;
     int y_off = L.y0, yt_off = L.yt;

@@ -52,18 +52,19 @@ __device__ __forceinline__ void reject_cell(const Grp<G>& g, const LaunchArgs& a
     }
 }
 
-// threads per CTA the kernel is compiled for
+// Registers per thread the kernel is compiled for: SLIM = 1, at most 128
+// (512 resident threads per SM); otherwise up to 255, except for 64 threads
+// per cell, capped at 200 so that five 64-thread CTAs fit an SM's registers
+// (their workspaces fit its shared memory: 45 KB each at 53 species).
 template <int G>
 struct PersistShape {
-    static constexpr int kThreads = G > 128 ? G : 128;
-    // SLIM = 1: at most 128 registers per thread (512 resident threads per SM)
-    static constexpr int kMinBlocksSlim = 512 / kThreads;
+    static constexpr int max_regs(int slim) { return slim ? 128 : (G == 64 ? 200 : 255); }
 };
 
 // NB: columns per LU panel; MS > 0: the matrix size m of every mechanism of
 // the launch, fixed at compile time (process_cell).
 template <int G, bool SHARED, int SLIM, int NB = 8, int MS = 0>
-__global__ void __launch_bounds__(PersistShape<G>::kThreads, SLIM ? PersistShape<G>::kMinBlocksSlim : 1)
+__global__ void __maxnreg__(PersistShape<G>::max_regs(SLIM))
     persistent_kernel(const MechSet P, const LaunchArgs a, int ws_per_cell, long long n_slots) {
     extern __shared__ double smem[];
     Grp<G> g;
