@@ -1461,10 +1461,11 @@ __device__ __forceinline__ void lu_solve_reg(const Grp<G>& g, const W& w, int A,
 }
 
 // Register form for one full warp with R rows per lane (m <= 32 R): lane l
-// holds rows l + 32 u. The steps run in tiles of 32 with the step index
-// unrolled, so the shuffle source lane, the tile and the row predicates are
-// compile-time and the loads of later steps can be issued early (the loop
-// stores nothing). Same operations and order as lu_solve_reg.
+// holds rows l + 32 u. The steps run in tiles of 32, the step loop unrolled by
+// 8 (full unrolling gives compile-time shuffle lanes and predicates, but its
+// code costs more in instruction fetch inside the solve kernel than it saves),
+// so the loads of later steps can be issued early (the loop stores nothing).
+// Same operations and order as lu_solve_reg.
 template <int R, class W>
 __device__ __forceinline__ void lu_solve_warp(const W& w, int A, int ld, int perm, int rdiag, int m, int b) {
     const int lane = threadIdx.x & 31;
@@ -1481,7 +1482,7 @@ __device__ __forceinline__ void lu_solve_warp(const W& w, int A, int ld, int per
 #pragma unroll
     for (int t = 0; t < R; ++t) {
         if (32 * t >= m - 1) break;
-#pragma unroll
+#pragma unroll 8
         for (int l = 0; l < 32; ++l) {
             const int j = 32 * t + l;
             if (j >= m - 1) break;
@@ -1496,7 +1497,7 @@ __device__ __forceinline__ void lu_solve_warp(const W& w, int A, int ld, int per
 #pragma unroll
     for (int t = R - 1; t >= 0; --t) {
         if (32 * t >= m) continue;
-#pragma unroll
+#pragma unroll 8
         for (int l = 31; l >= 0; --l) {
             const int j = 32 * t + l;
             if (j >= m) continue;
