@@ -81,8 +81,9 @@ def candidates(max_ws_doubles: int) -> List[dict]:
                 # the tuned variants (gf_solver_set_launch refuses those that do
                 # not apply to the solver's mechanisms; tune() skips them)
                 regs = 1 if G == 128 else 0
-                out.append(dict(kind=1, threads_per_cell=G, scratch_in_shared=shared, cells_per_block=0,
-                                blocks_per_sm=0, register_budget=regs, lu_panel=0, specialize=1))
+                for nb in (0, 4):
+                    out.append(dict(kind=1, threads_per_cell=G, scratch_in_shared=shared, cells_per_block=0,
+                                    blocks_per_sm=0, register_budget=regs, lu_panel=nb, specialize=1))
                 if shared:
                     for nb in (4, 16):
                         out.append(dict(kind=1, threads_per_cell=G, scratch_in_shared=1, cells_per_block=0,

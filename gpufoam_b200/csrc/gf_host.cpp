@@ -678,17 +678,10 @@ int gf_solver_set_launch(gf_solver* s, const gf_launch_config* cfg) {
         if (cfg->lu_panel != 0 && cfg->lu_panel != 4 && cfg->lu_panel != 8 && cfg->lu_panel != 16)
             return GF_ERR_INVALID_ARGUMENT;
         if (cfg->specialize != 0 && cfg->specialize != 1) return GF_ERR_INVALID_ARGUMENT;
-        // the tuned variants: 32, 64 and 128 threads, the form's usual register
-        // budget, panels of 4 or 16 columns in shared memory, or a compile-time
-        // matrix size every mechanism of the solver has
-        const bool panel = cfg->lu_panel == 4 || cfg->lu_panel == 16;
-        if (panel || cfg->specialize) {
-            if ((G != 32 && G != 64 && G != 128) || cfg->register_budget != (G == 128 ? 1 : 0))
-                return GF_ERR_UNSUPPORTED;
-            if (panel && (cfg->specialize || !cfg->scratch_in_shared)) return GF_ERR_UNSUPPORTED;
-            if (cfg->specialize && gf::specialized_size(s->dmechs.data(), (int)s->dmechs.size()) == 0)
-                return GF_ERR_UNSUPPORTED;
-        }
+        // the tuned variants (lu_panel 4 / 16, specialize) exist for some forms
+        // only (gf_persist.cuh, persistent_tuned_variant)
+        if (!gf::persistent_form_compiled(*cfg, gf::specialized_size(s->dmechs.data(), (int)s->dmechs.size())))
+            return GF_ERR_UNSUPPORTED;
     }
     s->cfg = *cfg;
     return GF_OK;

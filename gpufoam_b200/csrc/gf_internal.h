@@ -220,6 +220,8 @@ int record_cuda_error(int cuda_error);
 int persistent_slots(const gf_launch_config& cfg, int ms, int smem_bytes_per_cell, int* blocks_out,
                      int* threads_out);
 int specialized_size(const DevMech* mechs, int n_mechs);
+// Whether the library compiles the persistent kernel of this launch form.
+bool persistent_form_compiled(const gf_launch_config& cfg, int ms);
 int device_sm_count();
 
 }  // namespace gf

@@ -230,6 +230,8 @@ static const void* persistent_fn(const gf_launch_config& cfg, int ms) {
     }
 }
 
+bool persistent_form_compiled(const gf_launch_config& cfg, int ms) { return persistent_fn(cfg, ms) != nullptr; }
+
 int persistent_slots(const gf_launch_config& cfg, int ms, int smem_bytes_per_cell, int* blocks_out,
                      int* threads_out) {
     const int G = cfg.threads_per_cell;

@@ -104,30 +104,34 @@ const void* persistent_variant(bool shared, int slim) {
 // The tuned variants of the 32-, 64- and 128-thread forms (gf_persist_g<G>_tuned.cu):
 // LU panels of 4 or 16 columns (workspace in shared memory), and the matrix
 // size fixed at compile time for the 10-, 53- and 100-species mechanisms
-// (m = 11, 54, 101; workspace in shared memory or HBM). Each with the register
-// budget the form is usually run with (SLIM for 128 threads); nullptr for a
-// variant that is not compiled.
+// (m = 11, 54, 101; workspace in shared memory or HBM; for m = 54 also with
+// 4-column panels). Each with the register budget the form is usually run with
+// (SLIM for 128 threads); nullptr for a variant that is not compiled.
 constexpr int kTunedSlim(int G) { return G == 128 ? 1 : 0; }
+template <int G, int S, int NB, int MS>
+const void* tuned_kernel(bool shared) {
+    return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, NB, MS>)
+                  : reinterpret_cast<const void*>(&persistent_kernel<G, false, S, NB, MS>);
+}
 template <int G>
 const void* persistent_tuned_variant(bool shared, int slim, int nb, int ms) {
     if (slim != kTunedSlim(G)) return nullptr;
     constexpr int S = kTunedSlim(G);
     if (ms == 0) {
         if (!shared) return nullptr;
-        if (nb == 4) return reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 4, 0>);
-        if (nb == 16) return reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 16, 0>);
+        if (nb == 4) return tuned_kernel<G, S, 4, 0>(true);
+        if (nb == 16) return tuned_kernel<G, S, 16, 0>(true);
+        return nullptr;
+    }
+    if (ms == 54) {
+        if (nb == 4) return tuned_kernel<G, S, 4, 54>(shared);
+        if (nb == 8) return tuned_kernel<G, S, 8, 54>(shared);
         return nullptr;
     }
     if (nb != 8) return nullptr;
-    switch (ms) {
-    case 11: return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 8, 11>)
-                           : reinterpret_cast<const void*>(&persistent_kernel<G, false, S, 8, 11>);
-    case 54: return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 8, 54>)
-                           : reinterpret_cast<const void*>(&persistent_kernel<G, false, S, 8, 54>);
-    case 101: return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, 8, 101>)
-                            : reinterpret_cast<const void*>(&persistent_kernel<G, false, S, 8, 101>);
-    default: return nullptr;
-    }
+    if (ms == 11) return tuned_kernel<G, S, 8, 11>(shared);
+    if (ms == 101) return tuned_kernel<G, S, 8, 101>(shared);
+    return nullptr;
 }
 
 // defined in gf_persist_g<G>.cu

@@ -151,8 +151,7 @@ typedef struct gf_launch_config {
     int register_budget;     /* persistent only: 0 = up to 255 registers per thread,
                                 1 = at most 128 (more resident cell groups)      */
     int lu_panel;            /* persistent, 32/64/128 threads per cell: columns per LU
-                                panel, 4, 8 or 16 (0 = 8); 4 and 16 with the workspace
-                                in shared memory                                 */
+                                panel, 4, 8 or 16 (0 = 8; see gf_solver_set_launch) */
     int specialize;          /* persistent, 32/64/128 threads per cell: 1 = the kernel
                                 compiled for the matrix size of the solver's
                                 mechanisms (10, 53 or 100 species; all the same)  */
@@ -195,8 +194,9 @@ int gf_solver_create(const gf_mech* const* mechs, int n_mechs, const gf_ode_inpu
 void gf_solver_destroy(gf_solver* solver);
 /* GF_ERR_UNSUPPORTED for a form the library does not compile: lu_panel 4/16 or
  * specialize need 32, 64 or 128 threads per cell with register_budget 1 for
- * 128 threads and 0 otherwise; lu_panel 4/16 with scratch_in_shared and
- * specialize 0; specialize a solver whose mechanisms share 10, 53 or 100 species. */
+ * 128 threads and 0 otherwise; without specialize, lu_panel 4/16 needs
+ * scratch_in_shared; specialize needs a solver whose mechanisms share 10, 53 or
+ * 100 species, with lu_panel 8 (or 0), or 4 for 53 species. */
 int gf_solver_set_launch(gf_solver* solver, const gf_launch_config* cfg);
 int gf_solver_get_launch(const gf_solver* solver, gf_launch_config* cfg);
 /* The per-cell workspace of the solve kernels (doubles: in shared memory or

@@ -57,9 +57,13 @@ def test_tuned_variants_parity(factory):
     for G in (32, 64, 128):
         regs = 1 if G == 128 else 0
         forms = [dict(specialize=1, scratch_in_shared=0)]
+        if raw.n_species == 53:
+            forms += [dict(specialize=1, lu_panel=4, scratch_in_shared=0)]
         if ws <= 227 * 1024:
             forms += [dict(specialize=1, scratch_in_shared=1), dict(lu_panel=4, scratch_in_shared=1),
                       dict(lu_panel=16, scratch_in_shared=1)]
+            if raw.n_species == 53:
+                forms += [dict(specialize=1, lu_panel=4, scratch_in_shared=1)]
         for f in forms:
             s = E.Solver([mech], ode)
             s.set_launch(kind=1, threads_per_cell=G, register_budget=regs, **f)
@@ -75,7 +79,7 @@ def test_tuned_variants_parity(factory):
     s = E.Solver([mech], ode)
     for bad in (dict(threads_per_cell=16, specialize=1), dict(threads_per_cell=64, register_budget=1, lu_panel=4),
                 dict(threads_per_cell=64, lu_panel=4, scratch_in_shared=0),
-                dict(threads_per_cell=64, lu_panel=16, specialize=1)):
+                dict(threads_per_cell=64, lu_panel=16, specialize=1), dict(threads_per_cell=256, lu_panel=4)):
         with pytest.raises(N.GfError, match="UNSUPPORTED"):
             s.set_launch(kind=1, **bad)
     cov = E.Mechanism(M.coverage(0))   # 12 species: no kernel compiled for m = 13
