@@ -107,6 +107,10 @@ def parse():
     ap.add_argument("--shared", type=int, default=1)
     ap.add_argument("--register-budget", type=int, default=0, choices=[0, 1],
                     help="persistent kernel: 0 = up to 255 registers per thread, 1 = at most 128")
+    ap.add_argument("--lu-panel", type=int, default=0, choices=[0, 4, 8, 16],
+                    help="persistent kernel, fixed launch: columns per LU panel (0 = 8)")
+    ap.add_argument("--specialize", type=int, default=0, choices=[0, 1],
+                    help="persistent kernel, fixed launch: the kernel compiled for the mechanism's matrix size")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=1,
                     help="timed steps of the plain-kernel leg over the whole batch (at most --steps), after "
@@ -443,7 +447,7 @@ def main():
 
     solver = E.Solver(mechs, ode)
     solver.set_launch(kind=1, threads_per_cell=args.threads_per_cell, scratch_in_shared=args.shared,
-                      register_budget=args.register_budget)
+                      register_budget=args.register_budget, lu_panel=args.lu_panel, specialize=args.specialize)
     tuned = None
     if args.launch != "fixed":
         from gpufoam_b200 import autotune

@@ -23,8 +23,15 @@ from tests.parity import assert_states_close, step_count_agreement
 
 pytestmark = pytest.mark.gpu
 
-# the form the benchmark runs on the GRI-size batches (the autotuner's pick)
-BENCH_FORM = dict(kind=1, threads_per_cell=64, scratch_in_shared=1, register_budget=0)
+# the forms the autotuner picks between on the GRI-size batches (the fastest
+# first: 128 threads, 4-column LU panels, the kernel compiled for m = 54)
+BENCH_FORMS = {
+    "g128-slim-panel4-m54": dict(kind=1, threads_per_cell=128, scratch_in_shared=1, register_budget=1, lu_panel=4,
+                                 specialize=1),
+    "g64-panel4-m54": dict(kind=1, threads_per_cell=64, scratch_in_shared=1, lu_panel=4, specialize=1),
+    "g64-panel4": dict(kind=1, threads_per_cell=64, scratch_in_shared=1, lu_panel=4),
+    "g64": dict(kind=1, threads_per_cell=64, scratch_in_shared=1, register_budget=0),
+}
 PLAIN = dict(kind=0)
 
 
@@ -79,7 +86,8 @@ def compare(got, ref, raw, what):
 ])
 def test_bench_batch_sample(torch, workload, edges):
     """A stratified 2048-cell sample of the benchmark batch (seed 1000, as the
-    single-GPU bench) in the benchmarked form and the plain form."""
+    single-GPU bench) in the forms the benchmark's autotuner picks between and
+    the plain form."""
     wl = bench.WORKLOADS[workload]
     batch = bench.make_batch(wl, seed=1000)
     raw = batch.raws[0]
@@ -95,7 +103,7 @@ def test_bench_batch_sample(torch, workload, edges):
     ref = Oracle(raw, "port").cells(ode_inputs(34), cells, wl["dT"], bench.DTC0)
     mech = E.Mechanism(raw)
     ode = E.OdeInputs("Rosenbrock34", absTol=1e-8, relTol=1e-4)
-    for name, form in (("benchmarked form", BENCH_FORM), ("plain", PLAIN)):
+    for name, form in list(BENCH_FORMS.items()) + [("plain", PLAIN)]:
         got = solve(torch, [mech], ode, cells, wl["dT"], form)
         compare(got, ref, raw, f"{workload} {name}")
 
