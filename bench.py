@@ -86,10 +86,12 @@ def metric_name(workload, solver):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of the
 # persistent kernel on the GRI-size mechanism, from one ncu capture of 4 096
-# cells (threads_per_cell 64, shared-memory workspace): 2 481 152 B read, 0 B
-# written (the outputs were still in L2 when the launch ended). Scaled by the
-# cell count for the same kernel on the larger GRI-size batches.
-NCU_DRAM_BYTES_PER_CELL_GRI = 2481152 / 4096
+# cells in the launch form below (profiles/persistent_kernel_g128_gri4k.md):
+# 3 185 152 B read, 146 944 B written. Scaled by the cell count for the same
+# kernel on the larger GRI-size batches (the per-cell inputs and outputs are
+# moved once, the tables stay in L2).
+NCU_DRAM_BYTES_PER_CELL_GRI = (3185152 + 146944) / 4096
+NCU_PROFILED_FORM = dict(threads_per_cell=128, register_budget=1, lu_panel=4, specialize=1)
 
 
 def parse():
@@ -601,7 +603,8 @@ def main():
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value,
                          "traffic": (NCU_DRAM_BYTES_PER_CELL_GRI * n
-                                     if wl.get("mech") == "gri" and solver.get_launch()["threads_per_cell"] == 64
+                                     if wl.get("mech") == "gri" and all(solver.get_launch()[k] == v
+                                                                        for k, v in NCU_PROFILED_FORM.items())
                                      else None),
                          "traffic_source": "ncu dram bytes of 4096 GRI-size cells, scaled per cell",
                          "algorithmic_bytes_per_launch": int(n * 2 * cells.shape[1] * 8),
