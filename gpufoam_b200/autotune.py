@@ -5,9 +5,9 @@ offers on a sample of the caller's cells and keeps the fastest:
 
   * plain: one thread per cell, HBM scratch (the reference's launch model);
   * persistent work queue with G = 1, 4, 8, 16, 32 threads per cell (groups
-    inside a warp) or 64, 128, 256 (one cell per CTA), the per-cell workspace in
+    inside a warp) or 64, 96, 128, 256 (one cell per CTA), the per-cell workspace in
     shared memory (when it fits) or in HBM, and two register budgets;
-  * for 32, 64 and 128 threads per cell, the tile and specialisation variants:
+  * for 32, 64, 96 and 128 threads per cell, the tile and specialisation variants:
     LU panels of 4 or 16 columns instead of 8, and the kernel compiled for the
     mechanism's matrix size (10-, 53- and 100-species mechanisms), which fixes
     the workspace offsets, loop bounds and the unrolled tiles' predicates.
@@ -70,17 +70,17 @@ def candidates(max_ws_doubles: int) -> List[dict]:
     ws = max_ws_doubles * 8
     out = [dict(kind=0, threads_per_cell=1, scratch_in_shared=0, cells_per_block=0, blocks_per_sm=0,
                 register_budget=0, lu_panel=0, specialize=0)]
-    for G in (1, 4, 8, 16, 32, 64, 128, 256):
+    for G in (1, 4, 8, 16, 32, 64, 96, 128, 256):
         groups_per_cta = max(1, 128 // G) if G <= 32 else 1
         shared_ok = ws * (1 if G <= 32 else groups_per_cta) <= 227 * 1024
         for shared in ((1, 0) if shared_ok else (0,)):
             for regs in (0, 1):
                 out.append(dict(kind=1, threads_per_cell=G, scratch_in_shared=shared, cells_per_block=0,
                                 blocks_per_sm=0, register_budget=regs, lu_panel=0, specialize=0))
-            if G in (32, 64, 128):
+            if G in (32, 64, 96, 128):
                 # the tuned variants (gf_solver_set_launch refuses those that do
                 # not apply to the solver's mechanisms; tune() skips them)
-                regs = 1 if G == 128 else 0
+                regs = 1 if G in (96, 128) else 0
                 for nb in (0, 4):
                     out.append(dict(kind=1, threads_per_cell=G, scratch_in_shared=shared, cells_per_block=0,
                                     blocks_per_sm=0, register_budget=regs, lu_panel=nb, specialize=1))

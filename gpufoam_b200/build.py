@@ -18,9 +18,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libgpufoam_b200.so")
 OBJ = os.path.join(os.path.dirname(HERE), "_build", "obj")
-GROUPS = [1, 2, 4, 8, 16, 32, 64, 128, 256]
+GROUPS = [1, 2, 4, 8, 16, 32, 64, 96, 128, 256]
 SOURCES = (["gf_host.cpp", "gf_kernels.cu", "gf_peak.cu", "gf_noalloc.cu", "gf_adjoint.cu", "gf_fields.cu", "gf_fieldio.cu"] +
-           [f"gf_persist_g{g}.cu" for g in GROUPS] + [f"gf_persist_g{g}_tuned.cu" for g in (32, 64, 128)])
+           [f"gf_persist_g{g}.cu" for g in GROUPS] + [f"gf_persist_g{g}_tuned.cu" for g in (32, 64, 96, 128)])
 HEADERS = ["gf_internal.h", "gf_device.cuh", "gf_persist.cuh", "gf_adjoint.cuh", os.path.join("..", "..", "include", "gpufoam_b200.h")]
 
 NVCC_FLAGS = [

@@ -415,7 +415,7 @@ __device__ void adj_reactions(const Grp<G>& g, const DevMech& M, const W& w, con
 // plus the third-body terms c_bar[i] += sum_t Mbar[t] eff[t][i].
 template <int G, class W>
 __device__ void adj_gather_c(const Grp<G>& g, const DevMech& M, const W& w, const WsC& wa, const AdjLayout& A) {
-    stream_gather(g, M.cst[log2_group(G)], wa, A.gq, A.dd);
+    stream_gather(g, M.cst[stream_index(G)], wa, A.gq, A.dd);
     g.sync();
     for (int i = g.lane; i < M.nS; i += G) {
         double acc = wa[A.cb + i] + wa[A.dd + i];
@@ -622,7 +622,7 @@ __device__ void adj_step(const Grp<G>& g, const DevMech& M, const W& w, const Ws
         jacobian(g, M, w, L, L.y0, p, true);
         // kept for the Jacobian term: the raw entries (from the Jacobian terms
         // in the staging slots), the converted Jacobian and dfdx
-        stream_gather2(g, M.jst[log2_group(G)], w, L.stage, wa, A.raw);
+        stream_gather2(g, M.jst[stream_index(G)], w, L.stage, wa, A.raw);
         for (int e = g.lane; e < m * ld; e += G) wa[A.Jc + e] = w[L.J + e];
         for (int i = g.lane; i < m; i += G) wa[A.dfc + i] = w[L.dfdx + i];
         g.sync();

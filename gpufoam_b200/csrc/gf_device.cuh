@@ -60,7 +60,7 @@ static inline int phase_cycles_local(unsigned long long* out, int reset) {
 #endif
 enum { PH_MIX = 0, PH_NMPOW, PH_OMEGA, PH_GATHER_RHS, PH_JPARAMS, PH_JROWS, PH_TROW, PH_SHIFT, PH_LU, PH_SOLVE,
        PH_ADJ_RXN, PH_ATTEMPT, PH_ADJ_RECOMPUTE, PH_ADJ_TSOLVE, PH_ADJ_VJP, PH_ADJ_JTERM, PH_LU_PANEL, PH_LU_U12,
-       PH_LU_TRAIL };
+       PH_LU_TRAIL, PH_LU_PERM };
 
 // ---------------------------------------------------------------- groups
 
@@ -71,7 +71,7 @@ __device__ __forceinline__ double* grp_red_buf() {
 }
 
 // G <= 32: G aligned lanes of one warp, several groups per warp/CTA.
-// G = 64, 128, 256: the whole CTA (one cell per CTA); barriers are
+// G = 64, 96, 128, 256: the whole CTA (one cell per CTA); barriers are
 // __syncthreads and reductions go through a small shared buffer, in a fixed
 // warp order (deterministic).
 template <int G>
@@ -79,6 +79,7 @@ struct Grp {
     static constexpr int W = G > 32 ? G / 32 : 1;  // warps in the group
     int lane;
     unsigned mask;
+    __device__ __forceinline__ int warp() const { return G > 32 ? lane >> 5 : 0; }  // warp in the group
     __device__ __forceinline__ Grp() {
         const int wl = threadIdx.x & 31;
         if constexpr (G >= 32) {
@@ -114,7 +115,7 @@ struct Grp {
         for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, L);
         if (G > 32) {
             double* b = grp_red_buf();
-            if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+            if ((threadIdx.x & 31) == 0) b[lane >> 5] = v;
             __syncthreads();
             v = b[0];
 #pragma unroll
@@ -130,7 +131,7 @@ struct Grp {
         for (int o = L / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o, L));
         if (G > 32) {
             double* b = grp_red_buf();
-            if ((threadIdx.x & 31) == 0) b[threadIdx.x >> 5] = v;
+            if ((threadIdx.x & 31) == 0) b[lane >> 5] = v;
             __syncthreads();
             v = b[0];
 #pragma unroll
@@ -167,6 +168,7 @@ template <class T>
 __device__ __forceinline__ T ldg(const T* p) {
     return __ldg(p);
 }
+
 
 // ------------------------------------------------------------ thermo
 
@@ -609,6 +611,8 @@ __device__ __forceinline__ void stage_omega(const Grp<G>& g, const DevMech& M, c
 }
 
 __host__ __device__ constexpr int log2_group(int G) { return G <= 1 ? 0 : 1 + log2_group(G / 2); }
+// The index of a group size's gather streams in DevMech (group_size_of).
+__host__ __device__ constexpr int stream_index(int G) { return G == 96 ? 9 : log2_group(G); }
 
 // Runs this thread's share of a gather stream (gf_internal.h, Stream):
 // dst[pos] = sum of coef * src[slot] over each entry's records, in order.
@@ -646,7 +650,7 @@ template <int G, class W>
 __device__ __forceinline__ void gather_rhs(const Grp<G>& g, const DevMech& M, const W& w, const WsLayout& L,
                                            int out_off, double rhoM, double CpM) {
     const int nS = M.nS;
-    stream_gather(g, M.dst[log2_group(G)], w, L.stage, out_off);
+    stream_gather(g, M.dst[stream_index(G)], w, L.stage, out_off);
     g.sync();
     double s_h = 0;
     for (int s = g.lane; s < nS; s += G) {
@@ -857,7 +861,7 @@ __device__ __forceinline__ void jacobian(const Grp<G>& g, const DevMech& M, cons
     GF_PH_BEGIN(g)
     // raw dN/dc, T-column and third-body terms of every entry (species rows x
     // species and T columns), one thread per entry, in the reference's order
-    stream_gather(g, M.jst[log2_group(G)], w, L.stage, L.J);
+    stream_gather(g, M.jst[stream_index(G)], w, L.stage, L.J);
     g.sync();
     // phase 3
     for (int s = g.lane; s < nS; s += G) {
@@ -1191,7 +1195,7 @@ template <int G, int NB, bool EXACT = false, class W>
 __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv,
                                                       int m) {
     constexpr int NWp = G > 32 ? G / 32 : 1;
-    const int wid = G > 32 ? (int)(threadIdx.x >> 5) : 0;
+    const int wid = g.warp();
     const int l = G > 32 ? (int)(threadIdx.x & 31) : g.lane;
     for (int k0 = 0; k0 < m; ) {
         const int kb = min(NB, m - k0);
@@ -1260,7 +1264,7 @@ __device__ __forceinline__ void lu_decompose_blocked(const Grp<G>& g, const W& w
         // trailing matrix are updated by all warps (lanes over columns, warps
         // over rows), each entry still receiving its updates in k order
         constexpr int NWp = G / 32;
-        const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+        const int wid = g.warp(), l = threadIdx.x & 31;
         for (int k0 = 0; k0 < m; k0 += NB) {
             const int kb = min(NB, m - k0);
             const int k1 = k0 + kb;
@@ -1363,10 +1367,23 @@ __device__ __forceinline__ void lu_solve(const Grp<G>& g, const W& w, int A, int
 
 // The row permutation LUBacksubstitute applies to a right-hand side (its
 // sequence of exchanges b[i] <-> b[piv[i]]) as one gather: rhs'[i] = b[perm[i]].
+// A group of 32 or more threads computes each position's source in parallel
+// (the exchanges undone in reverse order: the row at position p came from
+// piv-exchange k applied to the source so far, k = m-1 .. 0); smaller groups
+// run the exchanges in order on one thread. Both give the same permutation.
 template <int G, class W>
 __device__ __forceinline__ void lu_perm(const Grp<G>& g, const W& w, int piv, int perm, int m) {
     g.sync();
-    if (g.lane == 0) {
+    if constexpr (G >= 32) {
+        for (int p = g.lane; p < m; p += G) {
+            int s = p;
+            for (int k = m - 1; k >= 0; --k) {
+                const int q = w.ip(piv + k);
+                s = s == k ? q : (s == q ? k : s);
+            }
+            w.ip(perm + p) = s;
+        }
+    } else if (g.lane == 0) {
         for (int i = 0; i < m; ++i) w.ip(perm + i) = i;
         for (int i = 0; i < m; ++i) {
             const int ip = w.ip(piv + i);
@@ -1524,7 +1541,7 @@ __device__ __forceinline__ void lu_solve_any(const Grp<G>& g, const W& w, int A,
         if (m <= 64) {
             g.sync();
             GF_PH_BEGIN(g)
-            if (G == 32 || threadIdx.x < 32) lu_solve_warp<2>(w, A, ld, perm, rdiag, m, b);
+            if (G == 32 || g.lane < 32) lu_solve_warp<2>(w, A, ld, perm, rdiag, m, b);
             g.sync();
             GF_PH_END(g, PH_SOLVE)
             return;
@@ -1560,8 +1577,10 @@ __device__ __forceinline__ void lu_factor(const Grp<G>& g, const W& w, int A, in
         GF_PH_END(g, PH_LU)
     }
     if (G >= 16) {
+        GF_PH_BEGIN(g)
         for (int i = g.lane; i < m; i += G) w[vv + i] = 1.0 / w[A + i * ld + i];
         lu_perm(g, w, piv, perm, m);
+        GF_PH_END(g, PH_LU_PERM)
     }
 }
 

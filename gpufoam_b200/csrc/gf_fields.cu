@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(32 * kFieldCellsMax) cell_fields_kernel(const 
         stage_fields(g, M, w, F.L, tcache, a.tc != nullptr, &sW, &sW2);
         g.sync();
         if (a.RR) {
-            stream_gather(g, M.dst[log2_group(32)], w, F.L.stage, F.out);
+            stream_gather(g, M.dst[stream_index(32)], w, F.L.stage, F.out);
             g.sync();
             double* rr = a.RR + cell * a.ld_rr;
             for (int i = g.lane; i < nS; i += 32) rr[i] = w[F.out + i] * ldg(M.W + i);

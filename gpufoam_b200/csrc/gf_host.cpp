@@ -477,9 +477,9 @@ int gf_mech_create(const gf_mech_desc* d, gf_mech** out) {
     std::vector<std::vector<StreamRec>> dst_rec(kNumGroupSizes), jst_rec(kNumGroupSizes), cst_rec(kNumGroupSizes);
     int dst_len[kNumGroupSizes], jst_len[kNumGroupSizes], cst_len[kNumGroupSizes];
     for (int k = 0; k < kNumGroupSizes; ++k) {
-        dst_rec[k] = build_stream(dn, dn_pos, 1 << k, &dst_len[k]);
-        jst_rec[k] = build_stream(je, je_pos, 1 << k, &jst_len[k]);
-        cst_rec[k] = build_stream(cg, dn_pos, 1 << k, &cst_len[k]);
+        dst_rec[k] = build_stream(dn, dn_pos, group_size_of(k), &dst_len[k]);
+        jst_rec[k] = build_stream(je, je_pos, group_size_of(k), &jst_len[k]);
+        cst_rec[k] = build_stream(cg, dn_pos, group_size_of(k), &cst_len[k]);
     }
     // keep every array non-empty
     if (eff.empty()) eff.push_back(0.0);
@@ -670,7 +670,7 @@ int gf_solver_set_launch(gf_solver* s, const gf_launch_config* cfg) {
     if (cfg->kind != 0 && cfg->kind != 1) return GF_ERR_INVALID_ARGUMENT;
     if (cfg->kind == 1) {
         const int G = cfg->threads_per_cell;
-        if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 128 && G != 256)
+        if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 96 && G != 128 && G != 256)
             return GF_ERR_INVALID_ARGUMENT;
         if (cfg->register_budget != 0 && cfg->register_budget != 1) return GF_ERR_INVALID_ARGUMENT;
         if (cfg->scratch_in_shared && (size_t)s->max_ws_doubles * sizeof(double) > 227 * 1024)

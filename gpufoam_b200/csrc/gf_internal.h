@@ -44,7 +44,8 @@ struct Stream {
     const StreamRec* rec;
     int len;  // records per thread (padded)
 };
-constexpr int kNumGroupSizes = 9;  // G = 1, 2, 4, ..., 256: stream index log2(G)
+constexpr int kNumGroupSizes = 10;  // G = 1, 2, 4, ..., 256: stream index log2(G); G = 96: index 9
+constexpr int group_size_of(int k) { return k < 9 ? 1 << k : 96; }
 
 // Device-resident mechanism tables. All arrays are device pointers; the struct
 // itself is passed to kernels by value.

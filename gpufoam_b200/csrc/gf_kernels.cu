@@ -200,7 +200,7 @@ int specialized_size(const DevMech* mechs, int n_mechs) {
 
 // The persistent kernel of a launch form: the generic variants of every group
 // size, or (lu_panel 4 / 16, or specialize with the matrix size ms) the tuned
-// variants of the 32-, 64- and 128-thread forms; nullptr if not compiled.
+// variants of the 32-, 64-, 96- and 128-thread forms; nullptr if not compiled.
 static const void* persistent_fn(const gf_launch_config& cfg, int ms) {
     const int G = cfg.threads_per_cell;
     const bool shared = cfg.scratch_in_shared != 0;
@@ -212,6 +212,7 @@ static const void* persistent_fn(const gf_launch_config& cfg, int ms) {
         switch (G) {
         case 32: return persistent_tuned_fn_g32(shared, slim, nb, sms);
         case 64: return persistent_tuned_fn_g64(shared, slim, nb, sms);
+        case 96: return persistent_tuned_fn_g96(shared, slim, nb, sms);
         case 128: return persistent_tuned_fn_g128(shared, slim, nb, sms);
         default: return nullptr;
         }
@@ -224,6 +225,7 @@ static const void* persistent_fn(const gf_launch_config& cfg, int ms) {
     case 16: return persistent_fn_g16(shared, slim);
     case 32: return persistent_fn_g32(shared, slim);
     case 64: return persistent_fn_g64(shared, slim);
+    case 96: return persistent_fn_g96(shared, slim);
     case 128: return persistent_fn_g128(shared, slim);
     case 256: return persistent_fn_g256(shared, slim);
     default: return nullptr;
@@ -253,19 +255,33 @@ int persistent_slots(const gf_launch_config& cfg, int ms, int smem_bytes_per_cel
         if (smem > 227 * 1024) return -2;
     }
     if (shared) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // shared-memory carveout: by default as much as the resident CTAs can use;
-    // with blocks_per_sm set, just enough for those CTAs, so that the rest of
-    // the SM's 256 KB serves as L1 for the mechanism tables
-    int carve = 100;
-    if (cfg.blocks_per_sm > 0) {
-        const size_t need = (size_t)cfg.blocks_per_sm * (smem + 1024) + 1024;
-        carve = (int)std::min<size_t>(100, (need * 100 + 228 * 1024 - 1) / (228 * 1024));
-    }
-    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    // shared-memory carveout: just enough for the CTAs that are resident
+    // (blocks_per_sm, or as many as registers, threads and shared memory allow
+    // at the largest carveout), so that the rest of the SM's 256 KB serves as
+    // L1 for the mechanism tables (with the workspace in HBM: for the
+    // workspaces too). The occupancy is taken again at the chosen carveout and
+    // the largest one kept if fewer CTAs would fit.
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) return -3;
     if (per_sm <= 0) return -4;
     if (cfg.blocks_per_sm > 0) per_sm = std::min(per_sm, cfg.blocks_per_sm);
+    {
+        int dev = 0, sm_max = 0, reserved = 0;
+        cudaFuncAttributes fa{};
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, fn) == cudaSuccess && sm_max > 0) {
+            const size_t need = (size_t)per_sm * (smem + fa.sharedSizeBytes + (size_t)reserved) + (size_t)reserved;
+            const int carve = (int)std::min<size_t>(100, (need * 100 + sm_max - 1) / (size_t)sm_max);
+            cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+            int again = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&again, fn, threads, smem) != cudaSuccess ||
+                again < per_sm)
+                cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        }
+    }
     const int blocks = per_sm * device_sm_count();
     *blocks_out = blocks;
     *threads_out = threads;
@@ -352,8 +368,13 @@ extern "C" int gf_debug_phase_cycles(unsigned long long* out, int reset) {
     phase_cycles_g16(out, reset);
     phase_cycles_g32(out, reset);
     phase_cycles_g64(out, reset);
+    phase_cycles_g96(out, reset);
     phase_cycles_g128(out, reset);
     phase_cycles_adj(out, reset);
+    phase_cycles_g32t(out, reset);
+    phase_cycles_g64t(out, reset);
+    phase_cycles_g96t(out, reset);
+    phase_cycles_g128t(out, reset);
     return phase_cycles_g256(out, reset);
 }
 namespace gf {

@@ -18,6 +18,7 @@ namespace gf {
 
 constexpr int kMaxMechs = 4;
 
+
 struct MechSet {
     DevMech m[kMaxMechs];
     int n;
@@ -101,13 +102,13 @@ const void* persistent_variant(bool shared, int slim) {
                 : reinterpret_cast<const void*>(&persistent_kernel<G, false, 0, NB, MS>);
 }
 
-// The tuned variants of the 32-, 64- and 128-thread forms (gf_persist_g<G>_tuned.cu):
+// The tuned variants of the 32-, 64-, 96- and 128-thread forms (gf_persist_g<G>_tuned.cu):
 // LU panels of 4 or 16 columns (workspace in shared memory), and the matrix
 // size fixed at compile time for the 10-, 53- and 100-species mechanisms
 // (m = 11, 54, 101; workspace in shared memory or HBM; for m = 54 also with
 // 4-column panels). Each with the register budget the form is usually run with
-// (SLIM for 128 threads); nullptr for a variant that is not compiled.
-constexpr int kTunedSlim(int G) { return G == 128 ? 1 : 0; }
+// (SLIM for 96 and 128 threads); nullptr for a variant that is not compiled.
+constexpr int kTunedSlim(int G) { return (G == 128 || G == 96) ? 1 : 0; }
 template <int G, int S, int NB, int MS>
 const void* tuned_kernel(bool shared) {
     return shared ? reinterpret_cast<const void*>(&persistent_kernel<G, true, S, NB, MS>)
@@ -142,11 +143,13 @@ const void* persistent_fn_g8(bool shared, int slim);
 const void* persistent_fn_g16(bool shared, int slim);
 const void* persistent_fn_g32(bool shared, int slim);
 const void* persistent_fn_g64(bool shared, int slim);
+const void* persistent_fn_g96(bool shared, int slim);
 const void* persistent_fn_g128(bool shared, int slim);
 const void* persistent_fn_g256(bool shared, int slim);
 // defined in gf_persist_g<G>_tuned.cu
 const void* persistent_tuned_fn_g32(bool shared, int slim, int nb, int ms);
 const void* persistent_tuned_fn_g64(bool shared, int slim, int nb, int ms);
+const void* persistent_tuned_fn_g96(bool shared, int slim, int nb, int ms);
 const void* persistent_tuned_fn_g128(bool shared, int slim, int nb, int ms);
 
 #ifdef GF_PHASE_TIMERS
@@ -158,9 +161,15 @@ int phase_cycles_g8(unsigned long long* out, int reset);
 int phase_cycles_g16(unsigned long long* out, int reset);
 int phase_cycles_g32(unsigned long long* out, int reset);
 int phase_cycles_g64(unsigned long long* out, int reset);
+int phase_cycles_g96(unsigned long long* out, int reset);
 int phase_cycles_g128(unsigned long long* out, int reset);
 int phase_cycles_g256(unsigned long long* out, int reset);
 int phase_cycles_adj(unsigned long long* out, int reset);
+// the tuned variants' units (gf_persist_g<G>_tuned.cu)
+int phase_cycles_g32t(unsigned long long* out, int reset);
+int phase_cycles_g64t(unsigned long long* out, int reset);
+int phase_cycles_g96t(unsigned long long* out, int reset);
+int phase_cycles_g128t(unsigned long long* out, int reset);
 #endif
 
 }  // namespace gf

@@ -6,4 +6,7 @@ namespace gf {
 const void* persistent_tuned_fn_g128(bool shared, int slim, int nb, int ms) {
     return persistent_tuned_variant<128>(shared, slim, nb, ms);
 }
+#ifdef GF_PHASE_TIMERS
+int phase_cycles_g128t(unsigned long long* out, int reset) { return phase_cycles_local(out, reset); }
+#endif
 }  // namespace gf

@@ -143,16 +143,16 @@ typedef struct gf_ode_inputs {
 typedef struct gf_launch_config {
     int kind;
     int threads_per_cell;    /* persistent only: 1, 2, 4, 8, 16, 32 (groups inside a
-                                warp) or 64, 128, 256 (one cell per CTA)         */
+                                warp) or 64, 96, 128, 256 (one cell per CTA)     */
     int scratch_in_shared;   /* 1: per-cell workspace in shared memory           */
     int cells_per_block;     /* groups per CTA (persistent, threads_per_cell <= 32;
                                 CTAs have at most 128 threads)                   */
     int blocks_per_sm;       /* 0 = as many as fit                               */
     int register_budget;     /* persistent only: 0 = up to 255 registers per thread,
                                 1 = at most 128 (more resident cell groups)      */
-    int lu_panel;            /* persistent, 32/64/128 threads per cell: columns per LU
+    int lu_panel;            /* persistent, 32/64/96/128 threads per cell: columns per LU
                                 panel, 4, 8 or 16 (0 = 8; see gf_solver_set_launch) */
-    int specialize;          /* persistent, 32/64/128 threads per cell: 1 = the kernel
+    int specialize;          /* persistent, 32/64/96/128 threads per cell: 1 = the kernel
                                 compiled for the matrix size of the solver's
                                 mechanisms (10, 53 or 100 species; all the same)  */
 } gf_launch_config;

@@ -1,6 +1,7 @@
 """gf_solve_noalloc: the solve for callers that cannot allocate device memory
-(CUDA-graph capture, foreign allocators, allocation-free loops). Its scratch is
-a static device array inside the library instead of memory from cudaMalloc.
+(a host code whose device memory belongs to another allocator, or a loop that
+forbids allocation once it has started). Its scratch is a static device array
+inside the library instead of memory from cudaMalloc.
 
 Compared through the C ABI with gf_solve on the same cells, for two calls in a
 row (the second call must not see state the first left in the shared array).
