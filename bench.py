@@ -87,10 +87,10 @@ def metric_name(workload, solver):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of the
 # persistent kernel on the GRI-size mechanism, from one ncu capture of 4 096
 # cells in the launch form below (profiles/persistent_kernel_g128_gri4k.md):
-# 3 020 032 B read, 99 072 B written. Scaled by the cell count for the same
+# 2 877 952 B read, 97 536 B written. Scaled by the cell count for the same
 # kernel on the larger GRI-size batches (the per-cell inputs and outputs are
 # moved once, the tables stay in L2).
-NCU_DRAM_BYTES_PER_CELL_GRI = (3020032 + 99072) / 4096
+NCU_DRAM_BYTES_PER_CELL_GRI = (2877952 + 97536) / 4096
 NCU_PROFILED_FORM = dict(threads_per_cell=128, register_budget=1, lu_panel=4, specialize=1)
 
 

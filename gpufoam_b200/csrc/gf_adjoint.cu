@@ -175,7 +175,7 @@ __device__ void lu_solve_transposed(const Grp<G>& g, const W& w, const WsC& wa, 
 template <int G, class WS, class WD>
 __device__ __forceinline__ void stream_gather2(const Grp<G>& g, const Stream& st, const WS& ws, int src, const WD& wd,
                                                int dst) {
-    constexpr int U = 8;
+    constexpr int U = GF_GATHER_BATCH;
     const int4* r = reinterpret_cast<const int4*>(st.rec) + g.lane;
     const int len = st.len;
     double acc = 0.0;

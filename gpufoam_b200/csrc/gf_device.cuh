@@ -62,6 +62,17 @@ enum { PH_MIX = 0, PH_NMPOW, PH_OMEGA, PH_GATHER_RHS, PH_JPARAMS, PH_JROWS, PH_T
        PH_ADJ_RXN, PH_ATTEMPT, PH_ADJ_RECOMPUTE, PH_ADJ_TSOLVE, PH_ADJ_VJP, PH_ADJ_JTERM, PH_LU_PANEL, PH_LU_U12,
        PH_LU_TRAIL, PH_LU_PERM };
 
+// Unroll depths of two latency-bound loops: third-body rows whose loads are in
+// flight together (third_body_all) and gather-stream records per batch
+// (stream_gather). 4 each: measured faster on the B200 than 8 (more loads in
+// flight, but more code to fetch inside the solve kernel) and than 2.
+#ifndef GF_TB_ROWS
+#define GF_TB_ROWS 4
+#endif
+#ifndef GF_GATHER_BATCH
+#define GF_GATHER_BATCH 4
+#endif
+
 // ---------------------------------------------------------------- groups
 
 // Cross-warp reduction buffer of a multi-warp group (one group per CTA).
@@ -376,14 +387,14 @@ __device__ __forceinline__ double arr_dlnkdT1(const DevMech& M, int q, const TCa
 // Third-body concentrations M_t = sum_i eff_ti c_i of every third-body and
 // fall-off reaction (gpuThirdBodyEfficiencies.H:28-35), written to Mtb[t]:
 // lanes over species (coalesced rows of eff), warps over reactions, rows in
-// batches of 8 so that their loads are in flight together; each sum is
+// batches of GF_TB_ROWS so that their loads are in flight together; each sum is
 // lane-strided and combined by a fixed shuffle tree (deterministic; the
 // reference sums sequentially, an ulp-level reordering).
 template <int G, class W>
 __device__ __forceinline__ void third_body_all(const Grp<G>& g, const DevMech& M, const W& w, int c_off, int m_off) {
     constexpr int LW = G > 32 ? 32 : G;
     constexpr int NW = G > 32 ? G / 32 : 1;
-    constexpr int RB = 8;
+    constexpr int RB = GF_TB_ROWS;
     constexpr int SPL = 3;  // species per lane held at once: nS <= SPL * LW, else looped
     const int rg = G > 32 ? (g.lane >> 5) : 0;
     const int rl = G > 32 ? (g.lane & 31) : g.lane;
@@ -620,7 +631,7 @@ __host__ __device__ constexpr int stream_index(int G) { return G == 96 ? 9 : log
 // they pipeline; one thread owns each output entry (no barriers inside).
 template <int G, class W>
 __device__ __forceinline__ void stream_gather(const Grp<G>& g, const Stream& st, const W& w, int src, int dst) {
-    constexpr int U = 8;  // records in flight per thread
+    constexpr int U = GF_GATHER_BATCH;  // records in flight per thread
     const int4* r = reinterpret_cast<const int4*>(st.rec) + g.lane;
     const int len = st.len;
     double acc = 0.0;
@@ -1479,10 +1490,14 @@ __device__ __forceinline__ void lu_solve_reg(const Grp<G>& g, const W& w, int A,
 
 // Register form for one full warp with R rows per lane (m <= 32 R): lane l
 // holds rows l + 32 u. The steps run in tiles of 32, the step loop unrolled by
-// 8 (full unrolling gives compile-time shuffle lanes and predicates, but its
-// code costs more in instruction fetch inside the solve kernel than it saves),
-// so the loads of later steps can be issued early (the loop stores nothing).
+// kSolveUnroll (4: measured faster than 8, 16 and full unrolling, whose code
+// costs more in instruction fetch inside the solve kernel than it saves), so
+// the loads of later steps can be issued early (the loop stores nothing).
 // Same operations and order as lu_solve_reg.
+#ifndef GF_SOLVE_UNROLL
+#define GF_SOLVE_UNROLL 4
+#endif
+constexpr int kSolveUnroll = GF_SOLVE_UNROLL;  // substitution steps unrolled together
 template <int R, class W>
 __device__ __forceinline__ void lu_solve_warp(const W& w, int A, int ld, int perm, int rdiag, int m, int b) {
     const int lane = threadIdx.x & 31;
@@ -1499,7 +1514,7 @@ __device__ __forceinline__ void lu_solve_warp(const W& w, int A, int ld, int per
 #pragma unroll
     for (int t = 0; t < R; ++t) {
         if (32 * t >= m - 1) break;
-#pragma unroll 8
+#pragma unroll kSolveUnroll
         for (int l = 0; l < 32; ++l) {
             const int j = 32 * t + l;
             if (j >= m - 1) break;
@@ -1514,7 +1529,7 @@ __device__ __forceinline__ void lu_solve_warp(const W& w, int A, int ld, int per
 #pragma unroll
     for (int t = R - 1; t >= 0; --t) {
         if (32 * t >= m) continue;
-#pragma unroll 8
+#pragma unroll kSolveUnroll
         for (int l = 31; l >= 0; --l) {
             const int j = 32 * t + l;
             if (j >= m) continue;

@@ -1127,7 +1127,7 @@ int gf_lu_decompose(int n_mats, int m, double* A, int* pivots, void* stream) {
 int gf_lu_factor_solve(int n_mats, int m, double* A, int* pivots, double* b, int n_rhs, int threads_per_matrix,
                        int exact, void* stream) {
     const int G = threads_per_matrix;
-    if (G != 1 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 128 && G != 256)
+    if (G != 1 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 96 && G != 128 && G != 256)
         return GF_ERR_INVALID_ARGUMENT;
     if (n_mats < 0 || m < 1 || m > 160 || n_rhs < 0 || (n_mats > 0 && (!A || !pivots || (n_rhs > 0 && !b))))
         return GF_ERR_INVALID_ARGUMENT;

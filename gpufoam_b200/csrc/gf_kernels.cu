@@ -173,6 +173,7 @@ int launch_lu_form(int n_mats, int m, double* A, int* piv, double* b, int n_rhs,
     case 16: return launch_lu_form_e<16>(n_mats, m, A, piv, b, n_rhs, exact, s);
     case 32: return launch_lu_form_e<32>(n_mats, m, A, piv, b, n_rhs, exact, s);
     case 64: return launch_lu_form_e<64>(n_mats, m, A, piv, b, n_rhs, exact, s);
+    case 96: return launch_lu_form_e<96>(n_mats, m, A, piv, b, n_rhs, exact, s);
     case 128: return launch_lu_form_e<128>(n_mats, m, A, piv, b, n_rhs, exact, s);
     case 256: return launch_lu_form_e<256>(n_mats, m, A, piv, b, n_rhs, exact, s);
     default: return (int)cudaErrorInvalidValue;

@@ -383,7 +383,7 @@ int gf_lu_backsubstitute(int n_mats, int m, const double* LU, const int* pivots,
                          double* b, void* stream);
 
 /* LUDecompose + LUBacksubstitute (ludecompose.H:9-130) as the solve kernels
- * run them, with threads_per_matrix (1, 4, 8, 16, 32, 64, 128 or 256) threads
+ * run them, with threads_per_matrix (1, 4, 8, 16, 32, 64, 96, 128 or 256) threads
  * per matrix: after the implicit row scaling, the register-panel factorisation
  * for 32 or more threads and m <= 64, the blocked one otherwise; solves by
  * reciprocal pivots for 16 or more threads. exact != 0 rounds every

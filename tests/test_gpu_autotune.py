@@ -23,7 +23,7 @@ def test_tuned_form_passes_parity():
     s = E.Solver([mech], ode)
     sample = M.make_cells(raw, 2048, seed=71)
     cands = [c for c in autotune.candidates(s.workspace_doubles())
-             if c["kind"] == 0 or c["threads_per_cell"] in (16, 32, 64, 128)]
+             if c["kind"] == 0 or c["threads_per_cell"] in (16, 32, 64, 96, 128)]
     res = autotune.tune(s, sample, 1e-6, configs=cands, use_cache=False)
     best = res["best"]
     assert s.get_launch() == best
@@ -54,8 +54,8 @@ def test_tuned_variants_parity(factory):
     dT = 1e-5 if raw.n_species <= 10 else 1e-6
     ref = Oracle(raw, "port").cells(ode_inputs(34), cells, dT, 1e-7)
     ws = E.Solver([mech], ode).workspace_doubles() * 8
-    for G in (32, 64, 128):
-        regs = 1 if G == 128 else 0
+    for G in (32, 64, 96, 128):
+        regs = 1 if G in (96, 128) else 0
         forms = [dict(specialize=1, scratch_in_shared=0)]
         if raw.n_species == 53:
             forms += [dict(specialize=1, lu_panel=4, scratch_in_shared=0)]

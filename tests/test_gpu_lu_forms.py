@@ -32,7 +32,7 @@ from gpufoam_b200 import evaluator as E
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lu_forms.npz")
-FORMS = [1, 4, 8, 16, 32, 64, 128, 256]
+FORMS = [1, 4, 8, 16, 32, 64, 96, 128, 256]
 
 
 @pytest.fixture(scope="module")

@@ -28,6 +28,7 @@ LAUNCHES = {
     "persist-g32-hbm": dict(kind=1, threads_per_cell=32, scratch_in_shared=0),
     "persist-g4-hbm": dict(kind=1, threads_per_cell=4, scratch_in_shared=0),
     "persist-g64-smem": dict(kind=1, threads_per_cell=64, scratch_in_shared=1),
+    "persist-g96-smem-slim": dict(kind=1, threads_per_cell=96, scratch_in_shared=1, register_budget=1),
     "persist-g128-smem-slim": dict(kind=1, threads_per_cell=128, scratch_in_shared=1, register_budget=1),
     "persist-g256-smem": dict(kind=1, threads_per_cell=256, scratch_in_shared=1),
     "persist-g128-hbm": dict(kind=1, threads_per_cell=128, scratch_in_shared=0),

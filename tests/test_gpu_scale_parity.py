@@ -28,6 +28,8 @@ pytestmark = pytest.mark.gpu
 BENCH_FORMS = {
     "g128-slim-panel4-m54": dict(kind=1, threads_per_cell=128, scratch_in_shared=1, register_budget=1, lu_panel=4,
                                  specialize=1),
+    "g96-slim-panel4-m54": dict(kind=1, threads_per_cell=96, scratch_in_shared=1, register_budget=1, lu_panel=4,
+                                specialize=1),
     "g64-panel4-m54": dict(kind=1, threads_per_cell=64, scratch_in_shared=1, lu_panel=4, specialize=1),
     "g64-panel4": dict(kind=1, threads_per_cell=64, scratch_in_shared=1, lu_panel=4),
     "g64": dict(kind=1, threads_per_cell=64, scratch_in_shared=1, register_budget=0),
