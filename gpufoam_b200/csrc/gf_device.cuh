@@ -1198,11 +1198,11 @@ __device__ __forceinline__ void lu_apply_swaps(const W& w, int A, int ld, int pi
 }
 
 // Register-panel form of the blocked LU for a full warp or a multi-warp group
-// (m <= 64): warp 0 factors each panel in registers; every column outside the
+// (m <= 32 RP, RP panel rows per lane): warp 0 factors each panel in registers; every column outside the
 // panel takes the panel's row exchanges, then (columns right of the panel) its
 // U12 rows; then the trailing matrix is updated (lanes over columns, warps over
 // rows). Every entry receives its updates in k order, as in lu_decompose.
-template <int G, int NB, bool EXACT = false, class W>
+template <int G, int NB, bool EXACT = false, int RP = 2, class W>
 __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& w, int A, int ld, int piv, int vv,
                                                       int m) {
     constexpr int NWp = G > 32 ? G / 32 : 1;
@@ -1215,7 +1215,7 @@ __device__ __forceinline__ void lu_decompose_regpanel(const Grp<G>& g, const W& 
             GF_PH_BEGIN(g)
             if (wid == 0) {
                 Grp<32> g32;
-                lu_panel_reg<2, NB, EXACT>(g32, w, A, ld, piv, vv, m, k0, k1);
+                lu_panel_reg<RP, NB, EXACT>(g32, w, A, ld, piv, vv, m, k0, k1);
             }
             g.sync();
             GF_PH_END(g, PH_LU_PANEL)
@@ -1420,7 +1420,7 @@ constexpr int kRegRows = 160;
 // permutation as a gather list (perm) or follow the pivots step by step (piv).
 template <int G>
 __host__ __device__ constexpr bool solve_uses_perm(int m) {
-    return (G >= 32 && m <= 64) || (G >= 16 && G <= 32 && m <= kRegRows);
+    return (G >= 32 && m <= 64) || (G > 32 && m <= 128) || (G >= 16 && G <= 32 && m <= kRegRows);
 }
 
 // The solve kernels' layout for a group of G threads: the pivot array the
@@ -1560,6 +1560,16 @@ __device__ __forceinline__ void lu_solve_any(const Grp<G>& g, const W& w, int A,
             g.sync();
             GF_PH_END(g, PH_SOLVE)
             return;
+        }
+        if constexpr (G > 32) {
+            // 64 < m <= 128 (the 100-species mechanism): four rows per lane,
+            // instead of the shared-memory form with a barrier per step
+            if (m <= 128) {
+                g.sync();
+                if (g.lane < 32) lu_solve_warp<4>(w, A, ld, perm, rdiag, m, b);
+                g.sync();
+                return;
+            }
         }
     }
     if constexpr (G >= 16 && G <= 32) {
